@@ -1,0 +1,372 @@
+#!/usr/bin/env python
+"""Benchmark of the LPS time marcher: node-steps/s on B200.
+
+Workload (default ``poisson7``): the Poisson-ratio batch -- seven instances of
+the Example 1 geometry (R=125 mm, dx=0.5 mm, m=4: 196,321 nodes, 6,268
+absorbing nodes, cloud size 49 each) with nu in {0.15,...,0.45}, a radial
+Gaussian pulse (A=1e-3 mm, sigma=40/3 mm), dt=17.5 ns, run together in one
+handle for 4000 time steps with diagnostics every 30 steps (the reference's
+output cadence, src/main.cpp:34,981).  One bench step = one complete run of
+the batch from its initial state.  Inputs are synthetic (lps_b200.gen):
+geometry, rings and clouds equal the reference preprocessor's; the absorbing
+operators are passive averaging operators of the same shape (the reference's
+least-squares fit is not restated).
+
+``--impl reference`` times the reference solver itself (compiled from its
+sources into oracle/_ref/, output off) on the host cores instead.
+
+Timing: W untimed bench steps, then K timed ones bracketed by a barrier and
+cuda synchronize, CUDA events on the solver's stream, max over ranks; L2 is
+flushed (256 MiB write) before every timed run, and the per-run working set
+(about 540 MB) exceeds L2 anyway.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "peridynamic-lps-absorbing-boundary_b200")
+sys.path.insert(0, PKG)
+
+METRIC = "node-steps/s on 1 B200: FP64 plain vs FP32-mixed batched at ≤1e-5 rel L2 err"
+NUS = (0.15, 0.20, 0.25, 0.30, 0.35, 0.40, 0.45)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["poisson7", "example1"], default="poisson7")
+    ap.add_argument("--time-steps", type=int, default=4000)
+    ap.add_argument("--diag-every", type=int, default=30)
+    ap.add_argument("--precision", default="fp64")
+    ap.add_argument("--path", default="auto")
+    ap.add_argument("--cpu-sample-steps", type=int, default=20)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload_sets(name, n_steps):
+    from lps_b200 import gen
+    nus = NUS if name == "poisson7" else (0.25,)
+    return [gen.disc_problem(R=125.0, dx=0.5, m=4, nu=nu, n_steps=n_steps) for nu in nus]
+
+
+def workload_config(name, sets, args):
+    return {"workload": ("Poisson-ratio batch: 7 x Example-1 disc (R=125 mm, dx=0.5 mm, m=4), "
+                         "nu 0.15..0.45" if name == "poisson7" else "Example 1 disc (R=125 mm, dx=0.5, m=4)"),
+            "instances": len(sets), "nodes_per_instance": sets[0].n_nodes,
+            "abc_nodes_per_instance": sets[0].n_abc, "cloud_size": sets[0].max_cloud,
+            "neighbours": 68, "time_steps_per_run": args.time_steps, "diag_every": args.diag_every,
+            "precision": args.precision, "path": args.path,
+            "l2": "flushed (256 MiB write) before each timed run; working set > L2"}
+
+
+# ---------------------------------------------------------------------------
+# CPU reference timing (the reference's own solver, compiled from its sources)
+def reference_cpu(s, n_steps, threads):
+    """Run oracle/_ref/PD2_LPS_ABC_timing on set s for n_steps; returns
+    (node_steps_per_s, seconds, kind) or None when the binary is missing."""
+    from lps_b200.files import write_input_set
+    binary = os.path.join(ROOT, "oracle", "_ref", "PD2_LPS_ABC_timing")
+    if not os.path.exists(binary):
+        return None
+    work = tempfile.mkdtemp(prefix="lps_ref_")
+    try:
+        s = _copy_steps(s, n_steps)
+        job = os.path.join(work, "ex")
+        write_input_set(job, s)
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+        r = subprocess.run([binary, "_t", "ex"], cwd=work, env=env, capture_output=True, text=True)
+        m = re.search(r"Time marching took ([0-9.eE+-]+) seconds", r.stdout)
+        if r.returncode != 0 or not m:
+            raise RuntimeError(f"reference solver failed: {r.stdout[-500:]} {r.stderr[-500:]}")
+        sec = float(m.group(1))
+        return s.n_nodes * n_steps / sec, sec
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+
+
+def _copy_steps(s, n_steps):
+    import copy
+    t = copy.copy(s)
+    t.n_steps = n_steps
+    return t
+
+
+def oracle_cpu(s, n_steps, threads):
+    """Fallback CPU leg: the C restatement (oracle/liblps_oracle.so)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_ctypes
+    r = oracle_ctypes.run(s, n_steps=n_steps, substep=10 ** 9, n_threads=threads)
+    return s.n_nodes * n_steps / r["elapsed"], r["elapsed"]
+
+
+def cpu_leg(s, n_steps, threads):
+    res = reference_cpu(s, n_steps, threads)
+    if res is not None:
+        return res + ("reference",)
+    return oracle_cpu(s, n_steps, threads) + ("port",)
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid):
+        self.uuid, self.proc, self.lines = uuid, None, []
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        cmd = ["nvidia-smi", f"--id={self.uuid}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+               "-lms", "200"]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.t = threading.Thread(target=self._read, daemon=True)
+        self.t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 7:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = float(f[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[3:7]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        return float(json.load(open(p))["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def algorithmic_bytes(sets, kernel):
+    """Compulsory bytes one launch of `kernel` moves (FP64 layout)."""
+    n = sum(s.n_nodes for s in sets)
+    abc = sum(s.n_abc * s.max_cloud for s in sets)
+    table = {
+        # pass 2: read u_pred 16, theta 8, m 8, v_half 16; write a 16, v 16 -- plus
+        # G_u, G_v (2 x 8C doubles) and the cloud indices (4C) per ABC node
+        "force": 80 * n + 132 * abc,
+        # pass 1: read u, v, a 48; write u_pred 16, v_half 16, theta 8 -- plus
+        # G_theta (2C doubles) and indices (4C) per ABC node
+        "theta": 88 * n + 20 * abc,
+        "predict": 80 * n,
+        "step": 168 * n + 152 * abc,
+    }
+    for k, v in table.items():
+        if kernel.startswith(k):
+            return v
+    return None
+
+
+# ---------------------------------------------------------------------------
+def run_ours(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from lps_b200.api import Solver
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    sets = workload_sets(args.workload, args.time_steps)
+    stream = torch.cuda.Stream(device=dev)
+    sv = Solver(sets, precision=args.precision, path=args.path, device=local_rank,
+                stream=stream.cuda_stream)
+    info = sv.info(0)
+    T, K, W = args.time_steps, args.steps, args.warmup
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    def one_run():
+        sv.reset()
+        sv.step(T, diag_every=args.diag_every)
+
+    for _ in range(W):
+        one_run()
+        for k in range(len(sets)):
+            sv.read_diag(k)
+    barrier()
+    clocks = ClockSampler(str(torch.cuda.get_device_properties(dev).uuid))
+    if rank == 0 or world > 1:
+        clocks.start()
+    launches0 = sv.kernel_launches
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    barrier()
+    for i in range(K):
+        with torch.cuda.stream(stream):
+            flush.fill_(float(i))
+        ev[i][0].record(stream)
+        one_run()
+        ev[i][1].record(stream)
+    barrier()
+    launches = sv.kernel_launches - launches0
+    clk = clocks.stop()
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    final_dE = []
+    for k in range(len(sets)):
+        d = sv.read_diag(k)
+        final_dE.append(float(d["dE_rel"][-1]) if len(d) else None)
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    node_steps = world * sum(s.n_nodes for s in sets) * T * K
+    value = node_steps / (ms_max / 1e3)
+
+    # ---- end to end through the C ABI: host inputs in, host results out ----
+    pin_u0 = [torch.from_numpy(np.ascontiguousarray(s.u0)).pin_memory() for s in sets]
+    pin_v0 = [torch.from_numpy(np.ascontiguousarray(s.v0)).pin_memory() for s in sets]
+    pin_out = [torch.empty(2 * s.n_nodes, dtype=torch.float64).pin_memory() for s in sets]
+    barrier()
+    t0 = time.perf_counter()
+    n_rec = 0
+    for _ in range(K):
+        for k in range(len(sets)):
+            sv.set_initial_ptr(k, pin_u0[k].data_ptr(), pin_v0[k].data_ptr())
+        sv.reset()
+        sv.step(T, diag_every=args.diag_every)
+        for k in range(len(sets)):
+            n_rec += len(sv.read_diag(k))
+            sv.download_u_ptr(k, pin_out[k].data_ptr())
+    barrier()
+    e2e_s = time.perf_counter() - t0
+    t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = node_steps / float(t.item())
+    h2d = sum(2 * 2 * s.n_nodes * 8 for s in sets)
+    d2h = sum(2 * s.n_nodes * 8 for s in sets) + (n_rec // K) * 128
+
+    # ---- per-kernel device times (live, CUDA events on the same stream) ----
+    sv.reset()
+    prof = sv.profile_kernels(120, diag_every=args.diag_every)
+    sv.close()
+    top = max(prof.items(), key=lambda kv: kv[1][1])
+    name, (nl, tot) = top
+    per_launch_ms = tot / nl
+    ab = algorithmic_bytes(sets, name)
+    peak, peak_kind = measured_peak_hbm()
+    achieved = ab / (per_launch_ms / 1e3) / 1e9 if ab else None
+    step_ms = sum(v[1] for v in prof.values()) / 120.0
+    roofline = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
+                "traffic": None, "algorithmic_bytes_per_launch": ab, "ms_per_launch": per_launch_ms,
+                "kernels": {k: {"launches": v[0], "ms_per_launch": v[1] / v[0]} for k, v in prof.items()},
+                "step_ms": step_ms,
+                "step_hbm_frac": (algorithmic_bytes(sets, "step") / (step_ms / 1e3) / 1e9) / peak}
+
+    out = {"metric": METRIC, "value": value, "unit": "node-steps/s", "n_gpus": world, "steps": K,
+           "warmup": W, "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+           "data": "synthetic (generated Example-1 geometry; passive averaging ABC operators)",
+           "config": workload_config(args.workload, sets, args) | {"parallelism": f"replicas{world}"},
+           "e2e": {"value": e2e_value, "unit": "node-steps/s", "h2d_bytes_per_step": h2d,
+                   "d2h_bytes_per_step": d2h},
+           "gpu_launches": launches, "roofline": roofline, "clocks": clk,
+           "kernel_path": info["path"], "final_dE_rel": final_dE}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        s_cpu = [s for s in sets if abs(s.nu - 0.25) < 1e-12][0] if len(sets) > 1 else sets[0]
+        v, sec, kind = cpu_leg(s_cpu, args.cpu_sample_steps, threads)
+        out["cpu_baseline"] = {"value": v, "unit": "node-steps/s", "cores": threads, "kind": kind,
+                               "sample": f"one nu=0.25 instance ({s_cpu.n_nodes} nodes), "
+                                         f"{args.cpu_sample_steps} time steps, output off, {sec:.2f} s"}
+    return out
+
+
+def run_reference(args):
+    """The reference's CPU solver on the same workload (bounded sample)."""
+    threads = os.cpu_count() or 1
+    sets = workload_sets(args.workload, args.time_steps)
+    per_step = args.cpu_sample_steps
+    n = per_step * (args.warmup + args.steps)
+    s = [t for t in sets if abs(t.nu - 0.25) < 1e-12][0]
+    v, sec, kind = cpu_leg(s, n, threads)
+    return {"metric": METRIC, "value": v, "unit": "node-steps/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * sec / (args.warmup + args.steps),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (generated Example-1 geometry; passive averaging ABC operators)",
+            "config": workload_config(args.workload, sets, args) | {"parallelism": "openmp"},
+            "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": "node-steps/s", "cores": threads, "kind": kind,
+                             "sample": f"one nu=0.25 instance ({s.n_nodes} nodes), {n} time steps "
+                                       f"({per_step} per bench step), output off, {sec:.2f} s"},
+            "e2e": {"value": v, "unit": "node-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local_rank))
+    out = run_ours(args, rank, world, local_rank)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

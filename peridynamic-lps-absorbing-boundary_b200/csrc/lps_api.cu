@@ -1,0 +1,930 @@
+// lps_api.cu -- the C ABI (include/lps_cuda.h): handle, batch packing, state
+// rings, CUDA-graph replay and the diagnostics log.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "lps_cuda.h"
+#include "lps_dense.cuh"
+#include "lps_kernels.cuh"
+#include "lps_setup.h"
+
+using namespace lps;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+template <class T>
+struct DevBuf {
+  T *p = nullptr;
+  size_t n = 0;
+};
+
+}  // namespace
+
+struct lps_handle {
+  lps_options opt{};
+  int n_inst = 0;
+  int path = LPS_PATH_CSR;
+  std::string err;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::vector<void *> allocs;
+  int64_t device_bytes = 0;
+
+  // per instance (host copies)
+  std::vector<InstanceSetup> setup;
+  std::vector<InstParams> params;
+  std::vector<int> node_begin, node_count, abc_begin, abc_count;
+  std::vector<double> E0;
+  std::vector<std::vector<DiagRecord>> drained;  // records pulled off the device, not yet read
+
+  // device layout
+  LaunchGeo lg{};
+  DenseGeo dg{};
+  int n_total = 0, n_abc_total = 0;
+  std::vector<int> local_of_global;  // for dense: cell -> local node index
+
+  // state
+  double2 *U[3] = {}, *V[3] = {}, *A[2] = {}, *VH = nullptr, *S = nullptr;
+  double *TH[3] = {};
+  double2 *U0 = nullptr, *V0 = nullptr;
+  // diagnostics
+  DiagPartial *partials = nullptr;
+  DiagRecord *log = nullptr;
+  int *log_count = nullptr;
+  int *d_step = nullptr;
+  int log_capacity = 0;
+  int pending_records = 0;  // records per instance on the device since the last drain
+
+  int64_t step = 0;          // steps taken since reset
+  int64_t launches = 0;
+  std::map<int, cudaGraphExec_t> graphs;  // key: 6-bit diag mask
+  std::map<int, int> graph_kernels;
+};
+
+namespace {
+
+const char *status_text(int s) {
+  switch (s) {
+    case LPS_OK: return "ok";
+    case LPS_ERR_INVALID_ARG: return "invalid argument";
+    case LPS_ERR_HORIZON: return "horizon longer than max_horizon";
+    case LPS_ERR_NONFINITE: return "energy or displacement is NaN/Inf";
+    case LPS_ERR_LAME: return "Lame parameter consistency check failed";
+    case LPS_ERR_LAMBDA_PD: return "lambda_PD consistency check failed";
+    case LPS_ERR_CUDA: return "CUDA error";
+    case LPS_ERR_NOMEM: return "out of memory";
+    case LPS_ERR_UNSUPPORTED: return "unsupported option combination";
+    case LPS_ERR_NO_DEVICE: return "no usable CUDA device";
+    default: return "unknown status";
+  }
+}
+
+#define LPS_CUDA_TRY(h, expr)                                                          \
+  do {                                                                                 \
+    cudaError_t e_ = (expr);                                                           \
+    if (e_ != cudaSuccess) {                                                           \
+      (h)->err = std::string(#expr) + ": " + cudaGetErrorString(e_);                  \
+      return LPS_ERR_CUDA;                                                             \
+    }                                                                                  \
+  } while (0)
+
+template <class T>
+int dev_alloc(lps_handle *h, T **p, size_t n) {
+  *p = nullptr;
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc((void **)p, n * sizeof(T));
+  if (e != cudaSuccess) {
+    h->err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? LPS_ERR_NOMEM : LPS_ERR_CUDA;
+  }
+  h->allocs.push_back(*p);
+  h->device_bytes += (int64_t)(n * sizeof(T));
+  return LPS_OK;
+}
+
+template <class T>
+int dev_upload(lps_handle *h, T **p, const std::vector<T> &v) {
+  int s = dev_alloc(h, p, v.size());
+  if (s) return s;
+  if (!v.empty()) LPS_CUDA_TRY(h, cudaMemcpy(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return LPS_OK;
+}
+
+inline int round_up(int x, int m) { return (x + m - 1) / m * m; }
+
+// ---------------------------------------------------------------------------
+// Batch packing shared by both paths: per-instance ABC lists.
+struct HostAbc {
+  std::vector<int> node, inst, cl_off, cl_len, cl_idx, idw_off, idw_len, idw_idx;
+  std::vector<uint8_t> writes, active;
+  std::vector<double> gu, gv, idw_w;
+  std::vector<double2> gth;
+};
+
+// Appends instance k's absorbing-boundary data.  `gmap(local)` maps a local
+// node index to the global node (or cell) index of the packed layout.
+template <class Map>
+void pack_abc(const lps_problem &p, const lps_options &o, const InstanceSetup &s, int k, Map gmap,
+              int begin, HostAbc &H, std::vector<int> &abc_of_global, std::vector<uint8_t> &type) {
+  const bool abc_on = o.abcs_step != -1 && p.n_abc > 0;
+  const int na = abc_on ? p.n_abc : 0;
+  const int C = p.max_cloud;
+  const int cpc = (o.abcs_step == 1) ? 2 : 4;       // G columns per cloud entry
+  const int cth = (o.abcs_step == 1) ? 1 : 2;       // G_theta columns per entry
+  const size_t cols = (size_t)cpc * C;
+  // the last active entry of a node is the one whose write survives
+  std::vector<int> last(p.n_nodes, -1);
+  for (int i = 0; i < na; i++)
+    if (p.bctypes[2 * p.inf_nodes[i]] == 1) last[p.inf_nodes[i]] = i;
+  for (int i = 0; i < na; i++) {
+    const int node = p.inf_nodes[i];
+    const int a = begin + i;
+    const bool active = p.bctypes[2 * node] == 1;
+    const bool writes = active && last[node] == i;
+    H.node[a] = gmap(node);
+    H.inst[a] = k;
+    H.active[a] = active;
+    H.writes[a] = writes;
+    H.cl_off[a] = (int)H.cl_idx.size();
+    int len = 0;
+    for (int j = 0; j < C; j++) {
+      const int kk = p.clouds[(size_t)i * C + j];
+      if (kk == -1) continue;
+      H.cl_idx.push_back(gmap(kk));
+      const double *g0 = p.gu + (size_t)(2 * i) * cols, *g1 = p.gu + (size_t)(2 * i + 1) * cols;
+      const double *h0 = p.gv + (size_t)(2 * i) * cols, *h1 = p.gv + (size_t)(2 * i + 1) * cols;
+      double gx[8] = {0, 0, 0, 0, 0, 0, 0, 0}, gy[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      for (int c = 0; c < cpc; c++) {
+        gx[c] = g0[cpc * j + c];
+        gx[4 + c] = g1[cpc * j + c];
+        gy[c] = h0[cpc * j + c];
+        gy[4 + c] = h1[cpc * j + c];
+      }
+      H.gu.insert(H.gu.end(), gx, gx + 8);
+      H.gv.insert(H.gv.end(), gy, gy + 8);
+      double2 w = make_double2(0.0, 0.0);
+      if (o.theta_method == 1 && p.gtheta) {
+        const double *gt = p.gtheta + (size_t)i * cth * C;
+        w.x = gt[cth * j];
+        if (cth == 2) w.y = gt[cth * j + 1];
+      }
+      H.gth.push_back(w);
+      len++;
+    }
+    H.cl_len[a] = len;
+    // inverse-distance lists, src/main.cpp:775-786
+    H.idw_off[a] = (int)H.idw_idx.size();
+    int il = 0;
+    if (writes && o.theta_method == 0) {
+      for (int j = 1; j < s.hz_len[node]; j++) {
+        const int nb = s.hz[(size_t)node * s.row_len + j];
+        if (nb == -1) continue;
+        if (p.bctypes[2 * nb] == 1) continue;
+        const double rx = p.nodes[2 * nb] - p.nodes[2 * node];
+        const double ry = p.nodes[2 * nb + 1] - p.nodes[2 * node + 1];
+        const double dist = std::sqrt(rx * rx + ry * ry);
+        H.idw_idx.push_back(gmap(nb));
+        H.idw_w.push_back(1.0 / (dist + 1e-30));
+        il++;
+      }
+    }
+    H.idw_len[a] = il;
+    if (writes) {
+      abc_of_global[gmap(node)] = a;
+      type[gmap(node)] |= kActiveAbc;
+    }
+  }
+}
+
+void fill_params(InstParams &P, const lps_problem &p, const lps_options &o, const InstanceSetup &s) {
+  memset(&P, 0, sizeof P);
+  P.dt = p.dt;
+  P.half_dt = p.dt / 2.0;
+  P.rho = p.rho;
+  P.lam = s.lam;
+  P.mu = s.mu;
+  P.kappa = s.kappa;
+  P.c_lm = 2.0 * (s.lam - s.mu);
+  P.c_mu8 = 8.0 * s.mu;
+  P.c_mu4 = 4.0 * s.mu;
+  P.dx = p.dx;
+  P.dy = p.dy;
+  P.delta = p.delta;
+  P.beta_lo = p.delta - p.dx / 2.0;
+  P.beta_hi = p.delta + p.dx / 2.0;
+  P.out_r = s.out_r;
+  P.kinematic = o.kinematic_v;
+  P.theta_method = o.theta_method;
+  P.abcs_step = o.abcs_step;
+}
+
+// ---------------------------------------------------------------------------
+int build_csr(lps_handle *h, const lps_problem *probs) {
+  const int K = h->n_inst;
+  // node ranges
+  int total = 0, total_abc = 0, width = 0;
+  for (int k = 0; k < K; k++) {
+    h->node_begin[k] = total;
+    h->node_count[k] = probs[k].n_nodes;
+    total += round_up(probs[k].n_nodes, kNodeBlock);
+    const bool abc_on = h->opt.abcs_step != -1 && probs[k].n_abc > 0;
+    h->abc_begin[k] = total_abc;
+    h->abc_count[k] = abc_on ? probs[k].n_abc : 0;
+    total_abc += round_up(h->abc_count[k], kNodeBlock);
+    width = std::max(width, h->setup[k].max_len - 1);
+  }
+  width = std::max(width, 1);
+  h->n_total = total;
+  h->n_abc_total = total_abc;
+  std::vector<double2> xy(total, make_double2(0, 0)), coef(total, make_double2(0, -1));
+  std::vector<uint8_t> type(total, 0);
+  std::vector<int> abc_of(total, -1), len(total, 0), nbr((size_t)width * total, -1);
+  std::vector<double> m(total, 0.0);
+  std::vector<int> blk_inst(total / kNodeBlock, 0);
+  HostAbc H;
+  H.node.assign(total_abc, 0); H.inst.assign(total_abc, 0);
+  H.cl_off.assign(total_abc, 0); H.cl_len.assign(total_abc, 0);
+  H.idw_off.assign(total_abc, 0); H.idw_len.assign(total_abc, 0);
+  H.writes.assign(total_abc, 0); H.active.assign(total_abc, 0);
+  for (int k = 0; k < K; k++) {
+    const lps_problem &p = probs[k];
+    const InstanceSetup &s = h->setup[k];
+    const int nb0 = h->node_begin[k];
+    for (int b = nb0 / kNodeBlock; b < (nb0 + round_up(p.n_nodes, kNodeBlock)) / kNodeBlock; b++) blk_inst[b] = k;
+    for (int i = 0; i < p.n_nodes; i++) {
+      const int g = nb0 + i;
+      xy[g] = make_double2(p.nodes[2 * i], p.nodes[2 * i + 1]);
+      type[g] = kExists | (p.bctypes[2 * i] == 1 ? kBcAbc : 0);
+      m[g] = s.m[i];
+      if (s.m[i] > 0.0)  // src/main.cpp:857-863 coefficients, same division
+        coef[g] = make_double2(2.0 * (s.lam - s.mu) / s.m[i], 8.0 * s.mu / s.m[i]);
+      int l = 0;
+      for (int j = 1; j < s.hz_len[i]; j++) {
+        const int nb = s.hz[(size_t)i * s.row_len + j];
+        nbr[(size_t)l * total + g] = nb < 0 ? -1 : nb0 + nb;
+        l++;
+      }
+      len[g] = l;
+    }
+    for (int a = h->abc_begin[k]; a < h->abc_begin[k] + round_up(h->abc_count[k], kNodeBlock); a++) {
+      H.inst[a] = k;
+      H.node[a] = nb0;
+    }
+    // padding entries keep writes = active = 0
+    pack_abc(p, h->opt, s, k, [nb0](int i) { return nb0 + i; }, h->abc_begin[k], H, abc_of, type);
+    fill_params(h->params[k], p, h->opt, s);
+    h->params[k].node_begin = nb0;
+    h->params[k].node_count = p.n_nodes;
+    h->params[k].abc_begin = h->abc_begin[k];
+    h->params[k].abc_count = h->abc_count[k];
+    int nact = 0;
+    for (int i = 0; i < h->abc_count[k]; i++) nact += p.bctypes[2 * p.inf_nodes[i]] == 1;
+    h->params[k].n_active_abc = nact;
+  }
+  // upload
+  Geo &G = h->lg.geo;
+  Abc &B = h->lg.abc;
+  G.n_total = total;
+  G.ell_width = width;
+  double2 *d_xy, *d_coef;
+  uint8_t *d_type;
+  int *d_abc_of, *d_len, *d_nbr, *d_blk;
+  double *d_m;
+  int s;
+  if ((s = dev_upload(h, &d_xy, xy)) || (s = dev_upload(h, &d_coef, coef)) ||
+      (s = dev_upload(h, &d_type, type)) || (s = dev_upload(h, &d_abc_of, abc_of)) ||
+      (s = dev_upload(h, &d_len, len)) || (s = dev_upload(h, &d_nbr, nbr)) ||
+      (s = dev_upload(h, &d_blk, blk_inst)) || (s = dev_upload(h, &d_m, m)))
+    return s;
+  G.xy = d_xy; G.coef = d_coef; G.type = d_type; G.abc_of = d_abc_of; G.len = d_len;
+  G.nbr = d_nbr; G.blk_inst = d_blk; G.m = d_m;
+  int *a_node, *a_inst, *a_cl_off, *a_cl_len, *a_cl_idx, *a_idw_off, *a_idw_len, *a_idw_idx;
+  uint8_t *a_writes, *a_active;
+  double *a_gu, *a_gv, *a_idw_w;
+  double2 *a_gth;
+  if ((s = dev_upload(h, &a_node, H.node)) || (s = dev_upload(h, &a_inst, H.inst)) ||
+      (s = dev_upload(h, &a_cl_off, H.cl_off)) || (s = dev_upload(h, &a_cl_len, H.cl_len)) ||
+      (s = dev_upload(h, &a_cl_idx, H.cl_idx)) || (s = dev_upload(h, &a_idw_off, H.idw_off)) ||
+      (s = dev_upload(h, &a_idw_len, H.idw_len)) || (s = dev_upload(h, &a_idw_idx, H.idw_idx)) ||
+      (s = dev_upload(h, &a_writes, H.writes)) || (s = dev_upload(h, &a_active, H.active)) ||
+      (s = dev_upload(h, &a_gu, H.gu)) || (s = dev_upload(h, &a_gv, H.gv)) ||
+      (s = dev_upload(h, &a_idw_w, H.idw_w)) || (s = dev_upload(h, &a_gth, H.gth)))
+    return s;
+  B.n_abc = total_abc;
+  B.node = a_node; B.inst = a_inst; B.cl_off = a_cl_off; B.cl_len = a_cl_len; B.cl_idx = a_cl_idx;
+  B.idw_off = a_idw_off; B.idw_len = a_idw_len; B.idw_idx = a_idw_idx; B.writes = a_writes;
+  B.active = a_active; B.gu = a_gu; B.gv = a_gv; B.idw_w = a_idw_w; B.gth = a_gth;
+  h->lg.n_node_blocks = total / kNodeBlock;
+  h->lg.n_abc_blocks = total_abc / kAbcWarpsPerBlock;
+  h->lg.n_inst = K;
+  h->lg.theta_method = h->opt.theta_method;
+  h->lg.abcs_step = h->opt.abcs_step;
+  return LPS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Ring indices of step s (1-based) whose current level is n = s - 1.
+StepPtrs step_ptrs(lps_handle *h, int64_t n) {
+  StepPtrs p;
+  const int u0 = (int)(n % 3), u1 = (int)((n + 1) % 3), um = (int)((n + 2) % 3);
+  const int a0 = (int)(n % 2), a1 = (int)((n + 1) % 2);
+  p.u_n = h->U[u0];
+  p.u_nm1 = h->U[um];
+  p.u_np1 = h->U[u1];
+  p.v_n = h->V[u0];
+  p.v_nm1 = h->V[um];
+  p.v_np1 = h->V[u1];
+  p.a_n = h->A[a0];
+  p.a_np1 = h->A[a1];
+  p.vh = h->VH;
+  p.th_n = h->TH[u0];
+  p.th_nm1 = h->TH[um];
+  p.th_np1 = h->TH[u1];
+  p.s_abc = h->S;
+  return p;
+}
+
+// Kernels of one step (and its diagnostics); returns the launch count.
+// `mark`, when set, is called after each launch with the kernel's name.
+int enqueue_step(lps_handle *h, int64_t n, bool diag, const Mark *mark = nullptr) {
+  const StepPtrs p = step_ptrs(h, n);
+  cudaStream_t st = h->stream;
+  auto M = [&](const char *name) {
+    if (mark) (*mark)(name);
+  };
+  int k = 0;
+  if (h->path == LPS_PATH_DENSE) {
+    k += enqueue_dense_step(h->dg, h->lg, p, h->d_step, st, mark);
+  } else {
+    launch_predict_csr(h->lg, p, st);
+    M("predict_csr");
+    launch_theta_csr(h->lg, p.u_np1, p.th_np1, p.th_n, p.th_nm1, true, st);
+    M("theta_csr");
+    k += 2;
+    if (h->opt.abcs_step != -1 && h->opt.theta_method == 0 && h->lg.abc.n_abc > 0) {
+      launch_theta_idw(h->lg, p.th_np1, st);
+      M("theta_idw");
+      k++;
+    }
+    launch_force_csr(h->lg, p, h->d_step, st);
+    M("force_csr");
+    k++;
+  }
+  if (diag) {
+    const bool abc = h->opt.abcs_step != -1 && h->lg.abc.n_abc > 0;
+    if (abc) {
+      launch_merge_abc(h->lg, p.u_np1, h->S, st);
+      M("merge_abc");
+      k++;
+    }
+    if (h->path == LPS_PATH_DENSE)
+      launch_diag_dense(h->dg, h->lg, p.u_np1, p.v_np1, p.a_np1, p.th_np1, h->partials, h->log,
+                        h->log_count, h->log_capacity, h->d_step, st);
+    else
+      launch_diag_csr(h->lg, p.u_np1, p.v_np1, p.a_np1, p.th_np1, h->partials, h->log, h->log_count,
+                      h->log_capacity, h->d_step, st);
+    M("diag");
+    k += 2;
+  }
+  return k;
+}
+
+int drain_log(lps_handle *h) {
+  if (h->pending_records == 0) return LPS_OK;
+  LPS_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  std::vector<int> cnt(h->n_inst);
+  LPS_CUDA_TRY(h, cudaMemcpy(cnt.data(), h->log_count, sizeof(int) * h->n_inst, cudaMemcpyDeviceToHost));
+  std::vector<DiagRecord> buf((size_t)h->n_inst * h->log_capacity);
+  LPS_CUDA_TRY(h, cudaMemcpy(buf.data(), h->log, sizeof(DiagRecord) * buf.size(), cudaMemcpyDeviceToHost));
+  for (int k = 0; k < h->n_inst; k++) {
+    const int c = std::min(cnt[k], h->log_capacity);
+    h->drained[k].insert(h->drained[k].end(), buf.begin() + (size_t)k * h->log_capacity,
+                         buf.begin() + (size_t)k * h->log_capacity + c);
+  }
+  LPS_CUDA_TRY(h, cudaMemsetAsync(h->log_count, 0, sizeof(int) * h->n_inst, h->stream));
+  h->pending_records = 0;
+  return LPS_OK;
+}
+
+int get_graph(lps_handle *h, int mask, cudaGraphExec_t *out) {
+  auto it = h->graphs.find(mask);
+  if (it != h->graphs.end()) {
+    *out = it->second;
+    return LPS_OK;
+  }
+  cudaGraph_t g;
+  LPS_CUDA_TRY(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  int kernels = 0;
+  for (int r = 0; r < 6; r++) kernels += enqueue_step(h, r, (mask >> r) & 1);
+  LPS_CUDA_TRY(h, cudaStreamEndCapture(h->stream, &g));
+  cudaGraphExec_t ex;
+  cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    h->err = std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e);
+    return LPS_ERR_CUDA;
+  }
+  h->graphs[mask] = ex;
+  h->graph_kernels[mask] = kernels;
+  *out = ex;
+  return LPS_OK;
+}
+
+__global__ void k_reset_state(int n, const double2 *u0, const double2 *v0, double2 *u_cur, double2 *u_prev,
+                              double2 *v_cur, double2 *v_prev, double2 *a_cur, double *th_prev) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  u_cur[i] = u0[i];
+  v_cur[i] = v0[i];
+  u_prev[i] = make_double2(0.0, 0.0);   // Unm1 = 0, src/main.cpp:632
+  v_prev[i] = make_double2(0.0, 0.0);   // Udnm1 = 0, :630
+  a_cur[i] = make_double2(0.0, 0.0);    // Uddn = 0, :628
+  th_prev[i] = 0.0;                     // ThetaNm1 = 0, :681
+}
+
+__global__ void k_reset_abc(Abc ab, const double2 *u0, double2 *s) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= ab.n_abc) return;
+  s[a] = ab.writes[a] ? u0[ab.node[a]] : make_double2(0.0, 0.0);
+}
+
+int do_reset(lps_handle *h) {
+  cudaStream_t st = h->stream;
+  const int n = h->n_total;
+  k_reset_state<<<(n + 255) / 256, 256, 0, st>>>(n, h->U0, h->V0, h->U[0], h->U[2], h->V[0], h->V[2],
+                                                  h->A[0], h->TH[2]);
+  LPS_CUDA_TRY(h, cudaMemsetAsync(h->TH[0], 0, sizeof(double) * n, st));
+  if (h->n_abc_total > 0)
+    k_reset_abc<<<(h->n_abc_total + 255) / 256, 256, 0, st>>>(h->lg.abc, h->U0, h->S);
+  // theta history from u^0 at every node (no override), src/main.cpp:664-682
+  if (h->opt.theta_method == 1) {
+    if (h->path == LPS_PATH_DENSE)
+      launch_theta_dense_init(h->dg, h->lg, h->U[0], h->TH[0], st);
+    else
+      launch_theta_csr(h->lg, h->U[0], h->TH[0], nullptr, nullptr, false, st);
+  }
+  LPS_CUDA_TRY(h, cudaMemsetAsync(h->d_step, 0, sizeof(int), st));
+  LPS_CUDA_TRY(h, cudaMemsetAsync(h->log_count, 0, sizeof(int) * h->n_inst, st));
+  LPS_CUDA_TRY(h, cudaGetLastError());
+  h->pending_records = 0;
+  h->step = 0;
+  for (int k = 0; k < h->n_inst; k++) {
+    h->E0[k] = -1.0;
+    h->drained[k].clear();
+  }
+  return LPS_OK;
+}
+
+int alloc_state(lps_handle *h) {
+  const int n = h->n_total;
+  int s;
+  for (int r = 0; r < 3; r++) {
+    if ((s = dev_alloc(h, &h->U[r], n)) || (s = dev_alloc(h, &h->V[r], n)) || (s = dev_alloc(h, &h->TH[r], n)))
+      return s;
+    LPS_CUDA_TRY(h, cudaMemset(h->U[r], 0, sizeof(double2) * n));
+    LPS_CUDA_TRY(h, cudaMemset(h->V[r], 0, sizeof(double2) * n));
+    LPS_CUDA_TRY(h, cudaMemset(h->TH[r], 0, sizeof(double) * n));
+  }
+  for (int r = 0; r < 2; r++) {
+    if ((s = dev_alloc(h, &h->A[r], n))) return s;
+    LPS_CUDA_TRY(h, cudaMemset(h->A[r], 0, sizeof(double2) * n));
+  }
+  if ((s = dev_alloc(h, &h->VH, n)) || (s = dev_alloc(h, &h->S, std::max(h->n_abc_total, 1))) ||
+      (s = dev_alloc(h, &h->U0, n)) || (s = dev_alloc(h, &h->V0, n)))
+    return s;
+  LPS_CUDA_TRY(h, cudaMemset(h->VH, 0, sizeof(double2) * n));
+  const int n_part = h->lg.n_node_blocks + (h->n_abc_total + kNodeBlock - 1) / kNodeBlock + 1;
+  h->log_capacity = 1024;
+  if ((s = dev_alloc(h, &h->partials, n_part)) ||
+      (s = dev_alloc(h, &h->log, (size_t)h->n_inst * h->log_capacity)) ||
+      (s = dev_alloc(h, &h->log_count, h->n_inst)) || (s = dev_alloc(h, &h->d_step, 1)))
+    return s;
+  return LPS_OK;
+}
+
+// Host-side interleaved (x,y) arrays -> node layout of the packed batch.
+void scatter_ic(lps_handle *h, int k, const double *src, std::vector<double2> &dst) {
+  const int n = h->node_count[k];
+  if (h->path == LPS_PATH_DENSE) {
+    const int *cell = h->dg.host_cell_of_node[k].data();
+    for (int i = 0; i < n; i++) dst[cell[i]] = make_double2(src[2 * i], src[2 * i + 1]);
+  } else {
+    const int b = h->node_begin[k];
+    for (int i = 0; i < n; i++) dst[b + i] = make_double2(src[2 * i], src[2 * i + 1]);
+  }
+}
+
+int global_of(const lps_handle *h, int k, int i) {
+  return h->path == LPS_PATH_DENSE ? h->dg.host_cell_of_node[k][i] : h->node_begin[k] + i;
+}
+
+void destroy_all(lps_handle *h) {
+  if (!h) return;
+  for (auto &g : h->graphs) cudaGraphExecDestroy(g.second);
+  h->graphs.clear();
+  for (void *p : h->allocs) cudaFree(p);
+  h->allocs.clear();
+  if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+  h->stream = nullptr;
+}
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+void lps_default_options(lps_options *o) {
+  if (!o) return;
+  memset(o, 0, sizeof *o);
+  o->abcs_step = 2;
+  o->theta_method = 1;
+  o->kinematic_v = 0;
+  o->max_horizon = 128;
+  o->precision = LPS_FP64;
+  o->path = LPS_PATH_AUTO;
+  o->device = 0;
+  o->use_graphs = 1;
+  o->stream = nullptr;
+}
+
+const char *lps_status_string(int s) { return status_text(s); }
+
+const char *lps_last_error(const lps_handle *h) {
+  return h ? h->err.c_str() : g_create_error.c_str();
+}
+
+int lps_create(const lps_problem *problems, int n_instances, const lps_options *opt, lps_handle **out) {
+  g_create_error.clear();
+  if (!out || !problems || n_instances <= 0 || n_instances > kMaxInstances) {
+    g_create_error = "lps_create: bad arguments (need 1..256 instances and an output pointer)";
+    return LPS_ERR_INVALID_ARG;
+  }
+  *out = nullptr;
+  lps_options o;
+  if (opt) o = *opt; else lps_default_options(&o);
+  if (o.max_horizon <= 1) o.max_horizon = 128;
+  if (o.precision != LPS_FP64) {
+    g_create_error = "lps_create: only the FP64 form is available in this build";
+    return LPS_ERR_UNSUPPORTED;
+  }
+  if (o.theta_method != 0 && o.theta_method != 1) {
+    g_create_error = "lps_create: theta_method must be 0 or 1";
+    return LPS_ERR_INVALID_ARG;
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0 || o.device < 0 || o.device >= ndev) {
+    g_create_error = "lps_create: no CUDA device";
+    return LPS_ERR_NO_DEVICE;
+  }
+  lps_handle *h = new lps_handle();
+  h->opt = o;
+  h->n_inst = n_instances;
+  h->device = o.device;
+  auto fail = [&](int s) {
+    g_create_error = h->err;
+    destroy_all(h);
+    delete h;
+    return s;
+  };
+  if (cudaSetDevice(o.device) != cudaSuccess) {
+    h->err = "cudaSetDevice failed";
+    return fail(LPS_ERR_NO_DEVICE);
+  }
+  {
+    cudaDeviceProp prop;
+    cudaGetDeviceProperties(&prop, o.device);
+    if (prop.major != 10) {
+      h->err = std::string("lps_create: this library is built for sm_100a; device is ") + prop.name;
+      return fail(LPS_ERR_NO_DEVICE);
+    }
+  }
+  if (o.stream) {
+    h->stream = (cudaStream_t)o.stream;
+  } else {
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      h->err = "cudaStreamCreate failed";
+      return fail(LPS_ERR_CUDA);
+    }
+    h->own_stream = true;
+  }
+  const int K = n_instances;
+  h->setup.resize(K);
+  h->params.resize(K);
+  h->node_begin.resize(K);
+  h->node_count.resize(K);
+  h->abc_begin.resize(K);
+  h->abc_count.resize(K);
+  h->E0.assign(K, -1.0);
+  h->drained.resize(K);
+  for (int k = 0; k < K; k++) {
+    int s = setup_instance(problems[k], o, h->setup[k], h->err);
+    if (s) {
+      if (K > 1) h->err = "instance " + std::to_string(k) + ": " + h->err;
+      return fail(s);
+    }
+  }
+  // path choice: dense when every instance maps onto a lattice
+  int s = LPS_OK;
+  bool dense_ok = o.path != LPS_PATH_CSR && dense_supported(problems, K, h->setup, o);
+  if (o.path == LPS_PATH_DENSE && !dense_ok) {
+    h->err = "lps_create: dense path requested but an instance is not a lattice";
+    return fail(LPS_ERR_UNSUPPORTED);
+  }
+  if (dense_ok) {
+    h->path = LPS_PATH_DENSE;
+    s = build_dense(h->dg, h->lg, problems, K, h->setup, o, h->params, h->node_begin, h->node_count,
+                    h->abc_begin, h->abc_count, h->n_total, h->n_abc_total, h->err,
+                    [h](void **p, size_t bytes) {
+                      cudaError_t e = cudaMalloc(p, bytes);
+                      if (e == cudaSuccess) {
+                        h->allocs.push_back(*p);
+                        h->device_bytes += (int64_t)bytes;
+                      }
+                      return e;
+                    });
+  } else {
+    h->path = LPS_PATH_CSR;
+    s = build_csr(h, problems);
+  }
+  if (s) return fail(s);
+  // per-instance constant table
+  if (upload_inst_params(h->params.data(), K, h->stream) != cudaSuccess) {
+    h->err = "upload of instance constants failed";
+    return fail(LPS_ERR_CUDA);
+  }
+  if ((s = alloc_state(h))) return fail(s);
+  // initial conditions
+  {
+    std::vector<double2> u0(h->n_total, make_double2(0, 0)), v0(h->n_total, make_double2(0, 0));
+    for (int k = 0; k < K; k++) {
+      scatter_ic(h, k, problems[k].u0, u0);
+      scatter_ic(h, k, problems[k].v0, v0);
+    }
+    if (cudaMemcpy(h->U0, u0.data(), sizeof(double2) * h->n_total, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(h->V0, v0.data(), sizeof(double2) * h->n_total, cudaMemcpyHostToDevice) != cudaSuccess) {
+      h->err = "upload of initial conditions failed";
+      return fail(LPS_ERR_CUDA);
+    }
+  }
+  if ((s = do_reset(h))) return fail(s);
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess) {
+    h->err = std::string("setup kernels failed: ") + cudaGetErrorString(cudaGetLastError());
+    return fail(LPS_ERR_CUDA);
+  }
+  *out = h;
+  return LPS_OK;
+}
+
+int lps_set_initial(lps_handle *h, int instance, const double *u0, const double *v0) {
+  if (!h || instance < 0 || instance >= h->n_inst) return LPS_ERR_INVALID_ARG;
+  const int n = h->node_count[instance];
+  std::vector<double2> buf;
+  for (int which = 0; which < 2; which++) {
+    const double *src = which == 0 ? u0 : v0;
+    if (!src) continue;
+    double2 *dst = which == 0 ? h->U0 : h->V0;
+    if (h->path == LPS_PATH_DENSE) {
+      // scatter on the host into the instance's cell range, then one copy
+      const int c0 = h->node_begin[instance], c1 = c0 + h->dg.host_cells[instance];
+      buf.assign(c1 - c0, make_double2(0, 0));
+      const int *cell = h->dg.host_cell_of_node[instance].data();
+      for (int i = 0; i < n; i++) buf[cell[i] - c0] = make_double2(src[2 * i], src[2 * i + 1]);
+      LPS_CUDA_TRY(h, cudaMemcpyAsync(dst + c0, buf.data(), sizeof(double2) * buf.size(),
+                                      cudaMemcpyHostToDevice, h->stream));
+      LPS_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    } else {
+      // the interleaved host layout is the device layout: one copy
+      LPS_CUDA_TRY(h, cudaMemcpyAsync(dst + h->node_begin[instance], src, sizeof(double2) * n,
+                                      cudaMemcpyHostToDevice, h->stream));
+    }
+  }
+  return LPS_OK;
+}
+
+int lps_reset(lps_handle *h) {
+  if (!h) return LPS_ERR_INVALID_ARG;
+  return do_reset(h);
+}
+
+int lps_step(lps_handle *h, int n_steps, int diag_every) {
+  if (!h || n_steps < 0) return LPS_ERR_INVALID_ARG;
+  int remaining = n_steps;
+  while (remaining > 0) {
+    // records this chunk adds per instance must fit in the device log
+    const int chunk = (h->step % 6 == 0 && remaining >= 6 && h->opt.use_graphs) ? 6 : 1;
+    int new_rec = 0, mask = 0;
+    for (int r = 0; r < chunk; r++) {
+      const int64_t s = h->step + 1 + r;
+      if (diag_every > 0 && s % diag_every == 0) {
+        mask |= 1 << r;
+        new_rec++;
+      }
+    }
+    if (h->pending_records + new_rec > h->log_capacity) {
+      int st = drain_log(h);
+      if (st) return st;
+    }
+    if (chunk == 6) {
+      cudaGraphExec_t ex;
+      int st = get_graph(h, mask, &ex);
+      if (st) return st;
+      LPS_CUDA_TRY(h, cudaGraphLaunch(ex, h->stream));
+      h->launches += h->graph_kernels[mask];
+    } else {
+      h->launches += enqueue_step(h, h->step, mask & 1);
+      LPS_CUDA_TRY(h, cudaGetLastError());
+    }
+    h->step += chunk;
+    h->pending_records += new_rec;
+    remaining -= chunk;
+  }
+  return LPS_OK;
+}
+
+int lps_read_diag(lps_handle *h, int instance, lps_diag *out, int max_records, int *n_records) {
+  if (!h || instance < 0 || instance >= h->n_inst || (max_records > 0 && !out)) return LPS_ERR_INVALID_ARG;
+  int st = drain_log(h);
+  if (st) return st;
+  LPS_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  std::vector<DiagRecord> &v = h->drained[instance];
+  const int n = std::min((int)v.size(), std::max(max_records, 0));
+  int status = LPS_OK;
+  for (int r = 0; r < n; r++) {
+    const DiagRecord &d = v[r];
+    lps_diag &o = out[r];
+    o.t = d.t; o.E = d.E; o.Ek = d.Ek; o.Ep = d.Ep; o.Px = d.Px; o.Py = d.Py;
+    o.max_u = d.max_u; o.max_v = d.max_v; o.max_a = d.max_a;
+    o.theta_min = d.th_min; o.theta_max = d.th_max;
+    o.uB_rms = d.nact > 0 ? std::sqrt(d.uB_sq / d.nact) : 0.0;   // src/main.cpp:1061-1062
+    o.vB_rms = d.nact > 0 ? std::sqrt(d.vB_sq / d.nact) : 0.0;
+    if (h->E0[instance] < 0.0) h->E0[instance] = d.E;                // :1046
+    const double E0 = h->E0[instance];
+    o.dE_rel = (E0 > 0.0) ? (d.E - E0) / E0 : 0.0;                  // :1047
+    o.step = d.step; o.max_u_node = d.iu; o.max_v_node = d.iv; o.n_active_abc = d.nact;
+    if (h->path == LPS_PATH_DENSE) {
+      o.max_u_node = d.iu >= 0 ? h->dg.host_node_of_cell(instance, d.iu) : -1;
+      o.max_v_node = d.iv >= 0 ? h->dg.host_node_of_cell(instance, d.iv) : -1;
+    }
+    if (std::isnan(d.E) || std::isinf(d.E) || std::isnan(d.max_u) || std::isinf(d.max_u)) {
+      status = LPS_ERR_NONFINITE;  // :1126-1133
+      h->err = "FATAL: Energy is NaN/Inf at step " + std::to_string(d.step) + "!";
+    }
+  }
+  v.erase(v.begin(), v.begin() + n);
+  if (n_records) *n_records = n;
+  return status;
+}
+
+int lps_download(lps_handle *h, int instance, double *u, double *v, double *a, double *theta, double *m) {
+  if (!h || instance < 0 || instance >= h->n_inst) return LPS_ERR_INVALID_ARG;
+  const int64_t n = h->step;
+  const StepPtrs p = step_ptrs(h, n > 0 ? n - 1 : 0);
+  // the newest level: after step n the current level is n
+  const int cur = (int)(n % 3), cura = (int)(n % 2);
+  if (h->opt.abcs_step != -1 && h->lg.abc.n_abc > 0) launch_merge_abc(h->lg, h->U[cur], h->S, h->stream);
+  (void)p;
+  LPS_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  const int nn = h->node_count[instance];
+  const int g0 = h->path == LPS_PATH_DENSE ? h->node_begin[instance] : h->node_begin[instance];
+  const int span = h->path == LPS_PATH_DENSE ? h->dg.host_cells[instance] : nn;
+  std::vector<double2> b2(span);
+  std::vector<double> b1(span);
+  auto get2 = [&](const double2 *src, double *dst) -> int {
+    if (!dst) return LPS_OK;
+    LPS_CUDA_TRY(h, cudaMemcpy(b2.data(), src + g0, sizeof(double2) * span, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < nn; i++) {
+      const int c = global_of(h, instance, i) - g0;
+      dst[2 * i] = b2[c].x;
+      dst[2 * i + 1] = b2[c].y;
+    }
+    return LPS_OK;
+  };
+  auto get1 = [&](const double *src, double *dst) -> int {
+    if (!dst) return LPS_OK;
+    LPS_CUDA_TRY(h, cudaMemcpy(b1.data(), src + g0, sizeof(double) * span, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < nn; i++) dst[i] = b1[global_of(h, instance, i) - g0];
+    return LPS_OK;
+  };
+  int s;
+  if ((s = get2(h->U[cur], u)) || (s = get2(h->V[cur], v)) || (s = get2(h->A[cura], a)) ||
+      (s = get1(h->TH[cur], theta)))
+    return s;
+  if (m) {
+    const InstanceSetup &su = h->setup[instance];
+    std::copy(su.m.begin(), su.m.end(), m);
+  }
+  return LPS_OK;
+}
+
+int lps_synchronize(lps_handle *h) {
+  if (!h) return LPS_ERR_INVALID_ARG;
+  LPS_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return LPS_OK;
+}
+
+int lps_get_info(lps_handle *h, int instance, lps_info *info) {
+  if (!h || !info || instance < 0 || instance >= h->n_inst) return LPS_ERR_INVALID_ARG;
+  memset(info, 0, sizeof *info);
+  const InstanceSetup &s = h->setup[instance];
+  info->n_instances = h->n_inst;
+  info->path = h->path;
+  info->precision = h->opt.precision;
+  info->max_horizon_len = s.max_len;
+  int64_t tn = 0, ta = 0;
+  for (int k = 0; k < h->n_inst; k++) {
+    tn += h->node_count[k];
+    ta += h->abc_count[k];
+  }
+  info->total_nodes = tn;
+  info->total_abc = ta;
+  info->m_ref = s.m_ref;
+  info->m_min = s.m_min;
+  info->lambda = s.lam;
+  info->mu = s.mu;
+  info->kappa = s.kappa;
+  info->alpha = s.alpha;
+  info->lambda_pd = s.lambda_pd;
+  info->output_exclude_r = s.out_r;
+  info->domain_radius = s.domain_radius;
+  info->dt_lps = s.dt_lps;
+  info->device_bytes = h->device_bytes;
+  info->step = h->step;
+  info->n_abc_m_corrected = s.n_corrected;
+  return LPS_OK;
+}
+
+int64_t lps_kernel_launches(const lps_handle *h) { return h ? h->launches : 0; }
+
+int lps_profile_kernels(lps_handle *h, int n_steps, int diag_every, lps_kernel_time *out, int max_kinds,
+                        int *n_kinds) {
+  if (!h || n_steps < 0 || (max_kinds > 0 && !out)) return LPS_ERR_INVALID_ARG;
+  std::vector<std::pair<std::string, cudaEvent_t>> ev;
+  cudaEvent_t start;
+  LPS_CUDA_TRY(h, cudaEventCreate(&start));
+  LPS_CUDA_TRY(h, cudaEventRecord(start, h->stream));
+  Mark mark = [&](const char *name) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    cudaEventRecord(e, h->stream);
+    ev.emplace_back(name, e);
+  };
+  for (int r = 0; r < n_steps; r++) {
+    const int64_t s = h->step + 1;
+    const bool diag = diag_every > 0 && s % diag_every == 0;
+    if (diag && h->pending_records + 1 > h->log_capacity) {
+      int st = drain_log(h);
+      if (st) return st;
+    }
+    h->launches += enqueue_step(h, h->step, diag, &mark);
+    h->step += 1;
+    h->pending_records += diag ? 1 : 0;
+  }
+  LPS_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  std::vector<std::string> names;
+  std::vector<double> ms;
+  std::vector<int> cnt;
+  cudaEvent_t prev = start;
+  for (auto &e : ev) {
+    float t = 0.f;
+    cudaEventElapsedTime(&t, prev, e.second);
+    prev = e.second;
+    auto it = std::find(names.begin(), names.end(), e.first);
+    if (it == names.end()) {
+      names.push_back(e.first);
+      ms.push_back(t);
+      cnt.push_back(1);
+    } else {
+      ms[it - names.begin()] += t;
+      cnt[it - names.begin()] += 1;
+    }
+  }
+  for (auto &e : ev) cudaEventDestroy(e.second);
+  cudaEventDestroy(start);
+  const int nk = std::min((int)names.size(), max_kinds);
+  for (int i = 0; i < nk; i++) {
+    memset(&out[i], 0, sizeof(lps_kernel_time));
+    strncpy(out[i].name, names[i].c_str(), sizeof(out[i].name) - 1);
+    out[i].launches = cnt[i];
+    out[i].total_ms = ms[i];
+  }
+  if (n_kinds) *n_kinds = nk;
+  return LPS_OK;
+}
+
+void lps_destroy(lps_handle *h) {
+  if (!h) return;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  destroy_all(h);
+  delete h;
+}
+
+}  // extern "C"

@@ -1,0 +1,151 @@
+"""Parity of the CUDA path (through the C ABI) with the reference and the oracle.
+
+Bars (the FP64 plain form): displacement and velocity relative L2 <= 1e-11
+after the run, the dE/E0 series within 1e-10 (relative once |dE/E0| > 1,
+which only the unstable r10 fixtures reach), weighted volumes bit-identical.
+Accelerations and dilatations are differences of nearly equal terms, so they
+are held to 1e-9 relative L2.
+"""
+import numpy as np
+import pytest
+
+import oracle_ctypes as O
+from golden_io import (ENERGY_COL, GOLDEN_CASES, VARIANT_OPTS, VERIFY_COL, inputs_for, load_golden,
+                       rel_l2)
+from lps_b200 import gen
+from lps_b200.api import LpsError, Solver
+
+pytestmark = pytest.mark.gpu
+
+STATE_TOL = 1e-11
+DERIVED_TOL = 1e-9
+DE_TOL = 1e-10
+PATHS = ["csr", "dense"]
+
+
+def run_gpu(s, path, n_steps=None, diag_every=1, **opts):
+    n = s.n_steps if n_steps is None else n_steps
+    with Solver(s, path=path, **opts) as sv:
+        sv.step(n, diag_every=diag_every)
+        d = sv.read_diag(0, check=False)
+        st = sv.download(0)
+        info = sv.info(0)
+        launches = sv.kernel_launches
+    return d, st, info, launches
+
+
+def check_series(d, en, ve):
+    E = en[:, ENERGY_COL["E"]]
+    assert np.max(np.abs(d["E"] - E) / np.abs(E)) <= 1e-11
+    dE = ve[:, VERIFY_COL["dE_rel"]]
+    assert np.max(np.abs(d["dE_rel"] - dE) / np.maximum(1.0, np.abs(dE))) <= DE_TOL
+    for name in ("Ek", "Ep"):
+        assert np.max(np.abs(d[name] - en[:, ENERGY_COL[name]])) <= 1e-11 * np.max(np.abs(E)), name
+    for name in ("max_u", "theta_max", "uB_rms", "vB_rms"):
+        ref = en[:, ENERGY_COL[name]]
+        assert np.max(np.abs(d[name] - ref)) <= 1e-9 * max(np.max(np.abs(ref)), 1e-300), name
+    for name in ("max_v", "max_a"):
+        ref = ve[:, VERIFY_COL[name]]
+        assert np.max(np.abs(d[name] - ref)) <= 1e-9 * np.max(np.abs(ref)), name
+
+
+@pytest.mark.parametrize("path", PATHS)
+@pytest.mark.parametrize("case,variant", GOLDEN_CASES, ids=[f"{c}_{v}" for c, v in GOLDEN_CASES])
+def test_golden_parity(case, variant, path):
+    """CUDA path vs the compiled reference's own outputs."""
+    s = inputs_for(case, variant)
+    g = load_golden(f"{case}_{variant}")
+    d, st, info, launches = run_gpu(s, path, **VARIANT_OPTS[variant])
+    assert info["path"] == path
+    assert launches >= 3 * s.n_steps
+    assert len(d) == s.n_steps
+    np.testing.assert_allclose(d["t"], g["energy"][:, 0], rtol=1e-15, atol=0)
+    for k in ("u", "v"):
+        assert rel_l2(st[k], g[k]) <= STATE_TOL, k
+    for k in ("a", "theta"):
+        assert rel_l2(st[k], g[k]) <= DERIVED_TOL, k
+    np.testing.assert_array_equal(st["m"], g["m"])
+    check_series(d, g["energy"], g["verify"])
+
+
+@pytest.mark.parametrize("path", PATHS)
+@pytest.mark.parametrize("m", [3, 4, 5, 8])
+def test_oracle_parity_generated(m, path):
+    """Generated discs (nu=0.3, passive averaging ABC) vs the oracle."""
+    s = gen.disc_problem(R=24.0, dx=0.5, m=m, nu=0.3, n_steps=240, sigma=4.0)
+    r = O.run(s, substep=20, max_horizon=256)
+    d, st, info, _ = run_gpu(s, path, diag_every=20, max_horizon=256)
+    assert r["status"] == 0
+    for k in ("u", "v"):
+        assert rel_l2(st[k], r[k]) <= STATE_TOL, k
+    for k in ("a", "theta"):
+        assert rel_l2(st[k], r[k]) <= DERIVED_TOL, k
+    dE = r["diag"]["dE_rel"]
+    assert np.max(np.abs(d["dE_rel"] - dE)) <= DE_TOL
+    np.testing.assert_array_equal(d["max_u_node"], r["diag"]["max_u_node"])
+
+
+@pytest.mark.parametrize("path", PATHS)
+def test_batch_equals_single(path):
+    """Uneven instances packed in one handle give each instance's own result."""
+    sets = [gen.disc_problem(R=12.0, m=4, nu=0.2, n_steps=60, sigma=3.0),
+            gen.disc_problem(R=20.0, m=3, nu=0.4, n_steps=60, sigma=5.0, centre=(2.0, -1.5)),
+            gen.disc_problem(R=9.0, m=5, nu=0.3, n_steps=60, sigma=2.0, abc="none")]
+    with Solver(sets, path=path) as sv:
+        sv.step(60, diag_every=6)
+        batch = [(sv.read_diag(k), sv.download(k)) for k in range(len(sets))]
+    for k, s in enumerate(sets):
+        d1, st1, _, _ = run_gpu(s, path, n_steps=60, diag_every=6)
+        for key in ("u", "v", "a", "theta"):
+            np.testing.assert_array_equal(batch[k][1][key], st1[key])
+        np.testing.assert_array_equal(batch[k][0]["E"], d1["E"])
+
+
+@pytest.mark.parametrize("path", PATHS)
+def test_graphs_match_eager(path):
+    s = gen.disc_problem(R=15.0, m=4, nu=0.35, n_steps=37, sigma=3.0)
+    d1, st1, _, _ = run_gpu(s, path, diag_every=5)
+    d2, st2, _, _ = run_gpu(s, path, diag_every=5, use_graphs=False)
+    for key in ("u", "v", "a", "theta"):
+        np.testing.assert_array_equal(st1[key], st2[key])
+    np.testing.assert_array_equal(d1["E"], d2["E"])
+
+
+def test_reset_and_set_initial_repeat():
+    s = gen.disc_problem(R=15.0, m=4, nu=0.3, n_steps=30, sigma=3.0)
+    with Solver(s) as sv:
+        sv.step(30, diag_every=10)
+        a = sv.download(0)
+        e1 = sv.read_diag(0)
+        sv.set_initial(0, s.u0 * 2.0, s.v0)
+        sv.reset()
+        sv.step(30, diag_every=10)
+        b = sv.download(0)
+        sv.read_diag(0)
+        sv.set_initial(0, s.u0, s.v0)
+        sv.reset()
+        sv.step(30, diag_every=10)
+        c = sv.download(0)
+        e3 = sv.read_diag(0)
+    assert rel_l2(b["u"], 2.0 * a["u"]) <= 1e-13   # linear system
+    np.testing.assert_array_equal(a["u"], c["u"])
+    np.testing.assert_array_equal(e1["E"], e3["E"])
+
+
+def test_nonfinite_initial_condition_is_fatal():
+    """A NaN in the initial displacement ends in the reference's FATAL status."""
+    s = gen.disc_problem(R=10.0, m=4, n_steps=10, sigma=3.0)
+    s.u0 = s.u0.copy()
+    s.u0[10] = np.nan
+    with Solver(s) as sv:
+        sv.step(10, diag_every=5)
+        with pytest.raises(LpsError) as e:
+            sv.read_diag(0)
+        assert e.value.status == -3
+
+
+def test_horizon_overflow_is_an_error():
+    s = gen.disc_problem(R=10.0, m=8, n_steps=1, abc="none")
+    with pytest.raises(LpsError) as e:
+        Solver(s, max_horizon=128)   # m=8: 225 entries with self
+    assert e.value.status == -2
