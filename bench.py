@@ -130,7 +130,9 @@ class ClockSampler:
          "clocks_event_reasons.sw_power_cap")
 
     def __init__(self, uuid):
-        self.uuid, self.proc, self.lines = uuid, None, []
+        uuid = str(uuid)
+        self.uuid = uuid if uuid.startswith("GPU-") else "GPU-" + uuid
+        self.proc, self.lines = None, []
 
     def start(self):
         if not shutil.which("nvidia-smi"):

@@ -226,6 +226,28 @@ void fill_params(InstParams &P, const lps_problem &p, const lps_options &o, cons
   P.abcs_step = o.abcs_step;
 }
 
+int upload_abc(lps_handle *h, const HostAbc &H, int total_abc) {
+  Abc &B = h->lg.abc;
+  int s;
+  int *a_node, *a_inst, *a_cl_off, *a_cl_len, *a_cl_idx, *a_idw_off, *a_idw_len, *a_idw_idx;
+  uint8_t *a_writes, *a_active;
+  double *a_gu, *a_gv, *a_idw_w;
+  double2 *a_gth;
+  if ((s = dev_upload(h, &a_node, H.node)) || (s = dev_upload(h, &a_inst, H.inst)) ||
+      (s = dev_upload(h, &a_cl_off, H.cl_off)) || (s = dev_upload(h, &a_cl_len, H.cl_len)) ||
+      (s = dev_upload(h, &a_cl_idx, H.cl_idx)) || (s = dev_upload(h, &a_idw_off, H.idw_off)) ||
+      (s = dev_upload(h, &a_idw_len, H.idw_len)) || (s = dev_upload(h, &a_idw_idx, H.idw_idx)) ||
+      (s = dev_upload(h, &a_writes, H.writes)) || (s = dev_upload(h, &a_active, H.active)) ||
+      (s = dev_upload(h, &a_gu, H.gu)) || (s = dev_upload(h, &a_gv, H.gv)) ||
+      (s = dev_upload(h, &a_idw_w, H.idw_w)) || (s = dev_upload(h, &a_gth, H.gth)))
+    return s;
+  B.n_abc = total_abc;
+  B.node = a_node; B.inst = a_inst; B.cl_off = a_cl_off; B.cl_len = a_cl_len; B.cl_idx = a_cl_idx;
+  B.idw_off = a_idw_off; B.idw_len = a_idw_len; B.idw_idx = a_idw_idx; B.writes = a_writes;
+  B.active = a_active; B.gu = a_gu; B.gv = a_gv; B.idw_w = a_idw_w; B.gth = a_gth;
+  return LPS_OK;
+}
+
 // ---------------------------------------------------------------------------
 int build_csr(lps_handle *h, const lps_problem *probs) {
   const int K = h->n_inst;
@@ -306,23 +328,240 @@ int build_csr(lps_handle *h, const lps_problem *probs) {
     return s;
   G.xy = d_xy; G.coef = d_coef; G.type = d_type; G.abc_of = d_abc_of; G.len = d_len;
   G.nbr = d_nbr; G.blk_inst = d_blk; G.m = d_m;
-  int *a_node, *a_inst, *a_cl_off, *a_cl_len, *a_cl_idx, *a_idw_off, *a_idw_len, *a_idw_idx;
-  uint8_t *a_writes, *a_active;
-  double *a_gu, *a_gv, *a_idw_w;
-  double2 *a_gth;
-  if ((s = dev_upload(h, &a_node, H.node)) || (s = dev_upload(h, &a_inst, H.inst)) ||
-      (s = dev_upload(h, &a_cl_off, H.cl_off)) || (s = dev_upload(h, &a_cl_len, H.cl_len)) ||
-      (s = dev_upload(h, &a_cl_idx, H.cl_idx)) || (s = dev_upload(h, &a_idw_off, H.idw_off)) ||
-      (s = dev_upload(h, &a_idw_len, H.idw_len)) || (s = dev_upload(h, &a_idw_idx, H.idw_idx)) ||
-      (s = dev_upload(h, &a_writes, H.writes)) || (s = dev_upload(h, &a_active, H.active)) ||
-      (s = dev_upload(h, &a_gu, H.gu)) || (s = dev_upload(h, &a_gv, H.gv)) ||
-      (s = dev_upload(h, &a_idw_w, H.idw_w)) || (s = dev_upload(h, &a_gth, H.gth)))
-    return s;
-  B.n_abc = total_abc;
-  B.node = a_node; B.inst = a_inst; B.cl_off = a_cl_off; B.cl_len = a_cl_len; B.cl_idx = a_cl_idx;
-  B.idw_off = a_idw_off; B.idw_len = a_idw_len; B.idw_idx = a_idw_idx; B.writes = a_writes;
-  B.active = a_active; B.gu = a_gu; B.gv = a_gv; B.idw_w = a_idw_w; B.gth = a_gth;
+  if ((s = upload_abc(h, H, total_abc))) return s;
   h->lg.n_node_blocks = total / kNodeBlock;
+  h->lg.n_abc_blocks = total_abc / kAbcWarpsPerBlock;
+  h->lg.n_inst = K;
+  h->lg.theta_method = h->opt.theta_method;
+  h->lg.abcs_step = h->opt.abcs_step;
+  return LPS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Dense path: lattice detection and the padded-grid layout.
+struct Lattice {
+  int M = 0, NR = 0, NC = 0;
+  std::vector<int> ix, iy;
+};
+
+// True when instance p sits exactly on a dx = dy lattice with delta = M dx,
+// M in kDenseM, no prenotch, and the reference's horizon search
+// (src/main.cpp:352) admits exactly the stencil offsets of M.
+bool lattice_of(const lps_problem &p, const InstanceSetup &s, Lattice &L) {
+  if (p.n_prenotch > 0 || p.dx != p.dy) return false;
+  const double mr = p.delta / p.dx;
+  const int M = (int)std::llround(mr);
+  if (M <= 0 || std::abs(mr - M) > 1e-12 * mr || !dense_m_supported(M)) return false;
+  std::vector<int> A, B;
+  dense_offsets(M, A, B);
+  const double r = p.delta + p.dx / 2.0 + 1e-5;
+  int admitted = 0;
+  for (int a = -M - 2; a <= M + 2; a++)
+    for (int b = -M - 2; b <= M + 2; b++) {
+      if (a == 0 && b == 0) continue;
+      const double x = a * p.dx, y = b * p.dy;
+      const bool in_ref = std::sqrt(x * x + y * y) <= r;
+      const bool in_sten = a * a + b * b <= M * M + M;
+      if (in_ref != in_sten) return false;
+      admitted += in_ref;
+    }
+  if (admitted != (int)A.size()) return false;
+  const int N = p.n_nodes;
+  double x0 = p.nodes[0], y0 = p.nodes[1];
+  for (int i = 1; i < N; i++) {
+    x0 = std::min(x0, p.nodes[2 * i]);
+    y0 = std::min(y0, p.nodes[2 * i + 1]);
+  }
+  L.M = M;
+  L.ix.resize(N);
+  L.iy.resize(N);
+  long mx = 0, my = 0;
+  for (int i = 0; i < N; i++) {
+    const double x = p.nodes[2 * i], y = p.nodes[2 * i + 1];
+    const long ix = std::lround((x - x0) / p.dx), iy = std::lround((y - y0) / p.dy);
+    if (std::abs(x0 + ix * p.dx - x) > 1e-13 * (std::abs(x) + std::abs(x0) + p.dx)) return false;
+    if (std::abs(y0 + iy * p.dy - y) > 1e-13 * (std::abs(y) + std::abs(y0) + p.dy)) return false;
+    if (ix > (1 << 20) || iy > (1 << 20)) return false;
+    L.ix[i] = (int)ix;
+    L.iy[i] = (int)iy;
+    mx = std::max(mx, ix);
+    my = std::max(my, iy);
+  }
+  L.NR = (int)mx + 1;
+  L.NC = (int)my + 1;
+  if ((double)L.NR * L.NC > 2.0e9) return false;
+  std::vector<int> seen((size_t)L.NR * L.NC, -1);
+  for (int i = 0; i < N; i++) {
+    int &c = seen[(size_t)L.ix[i] * L.NC + L.iy[i]];
+    if (c >= 0) return false;  // two nodes in one cell
+    c = i;
+  }
+  // the host horizons must be exactly the existing stencil neighbours
+  for (int i = 0; i < N; i++) {
+    int cnt = 1;
+    for (size_t j = 0; j < A.size(); j++) {
+      const long jx = L.ix[i] + A[j], jy = L.iy[i] + B[j];
+      if (jx >= 0 && jx < L.NR && jy >= 0 && jy < L.NC && seen[(size_t)jx * L.NC + jy] >= 0) cnt++;
+    }
+    if (cnt != s.hz_len[i]) return false;
+  }
+  return true;
+}
+
+bool dense_possible(const lps_problem *probs, int K, const std::vector<InstanceSetup> &setup,
+                    std::vector<Lattice> &lat) {
+  lat.assign(K, Lattice());
+  std::map<int, std::pair<double, double>> spacing;  // one constant set per M
+  for (int k = 0; k < K; k++) {
+    if (!lattice_of(probs[k], setup[k], lat[k])) return false;
+    auto it = spacing.find(lat[k].M);
+    if (it == spacing.end())
+      spacing[lat[k].M] = {probs[k].dx, probs[k].delta};
+    else if (it->second.first != probs[k].dx || it->second.second != probs[k].delta)
+      return false;
+  }
+  return true;
+}
+
+int build_dense(lps_handle *h, const lps_problem *probs, const std::vector<Lattice> &lat) {
+  const int K = h->n_inst;
+  DenseGeo &D = h->dg;
+  D.host_cell_of_node.assign(K, {});
+  D.host_node_of_cell_v.assign(K, {});
+  D.host_cells.assign(K, 0);
+  D.host_cell_begin.assign(K, 0);
+  std::vector<int> pitch(K), rows(K), cols(K);
+  long total = 0;
+  int total_abc = 0;
+  for (int k = 0; k < K; k++) {
+    const int M = lat[k].M;
+    const int NRt = round_up(lat[k].NR, kTileRows), NCt = round_up(lat[k].NC, kTileCols);
+    rows[k] = NRt + 2 * M;
+    cols[k] = NCt;
+    pitch[k] = round_up(NCt + 2 * M, 8);
+    const long cells = (long)round_up(rows[k] * pitch[k], kNodeBlock);
+    D.host_cell_begin[k] = (int)total;
+    D.host_cells[k] = (int)cells;
+    h->node_begin[k] = (int)total;
+    h->node_count[k] = probs[k].n_nodes;
+    total += cells;
+    const bool abc_on = h->opt.abcs_step != -1 && probs[k].n_abc > 0;
+    h->abc_begin[k] = total_abc;
+    h->abc_count[k] = abc_on ? probs[k].n_abc : 0;
+    total_abc += round_up(h->abc_count[k], kNodeBlock);
+  }
+  if (total > 2000000000L) {
+    h->err = "lps_create: dense layout larger than 2^31 cells";
+    return LPS_ERR_UNSUPPORTED;
+  }
+  const int n = (int)total;
+  h->n_total = n;
+  h->n_abc_total = total_abc;
+  std::vector<double2> xy(n, make_double2(0, 0)), coef(n, make_double2(0, -1));
+  std::vector<uint8_t> type(n, 0);
+  std::vector<int> abc_of(n, -1), blk_inst(n / kNodeBlock, 0);
+  std::vector<double> m(n, 0.0);
+  HostAbc H;
+  H.node.assign(total_abc, 0); H.inst.assign(total_abc, 0);
+  H.cl_off.assign(total_abc, 0); H.cl_len.assign(total_abc, 0);
+  H.idw_off.assign(total_abc, 0); H.idw_len.assign(total_abc, 0);
+  H.writes.assign(total_abc, 0); H.active.assign(total_abc, 0);
+  std::vector<DenseTile> tiles;
+  for (int k = 0; k < K; k++) {
+    const lps_problem &p = probs[k];
+    const InstanceSetup &s = h->setup[k];
+    const int M = lat[k].M, P = pitch[k], c0 = D.host_cell_begin[k];
+    for (int b = c0 / kNodeBlock; b < (c0 + D.host_cells[k]) / kNodeBlock; b++) blk_inst[b] = k;
+    auto &cell_of = D.host_cell_of_node[k];
+    auto &node_of = D.host_node_of_cell_v[k];
+    cell_of.resize(p.n_nodes);
+    node_of.assign(D.host_cells[k], -1);
+    for (int i = 0; i < p.n_nodes; i++) {
+      const int c = c0 + (lat[k].ix[i] + M) * P + (lat[k].iy[i] + M);
+      cell_of[i] = c;
+      node_of[c - c0] = i;
+      xy[c] = make_double2(p.nodes[2 * i], p.nodes[2 * i + 1]);
+      type[c] = kExists | (p.bctypes[2 * i] == 1 ? kBcAbc : 0);
+      m[c] = s.m[i];
+      if (s.m[i] > 0.0) coef[c] = make_double2(2.0 * (s.lam - s.mu) / s.m[i], 8.0 * s.mu / s.m[i]);
+    }
+    // tiles: owned rows [r0, r0 + 16), columns [c, c + 32) of the lattice
+    std::vector<int> A, B;
+    dense_offsets(M, A, B);
+    const int NRt = rows[k] - 2 * M;
+    for (int r0 = 0; r0 < NRt; r0 += kTileRows)
+      for (int q0 = 0; q0 < cols[k]; q0 += kTileCols) {
+        const int base = c0 + (r0 + M) * P + (q0 + M);
+        bool any = false, full = true;
+        for (int r = 0; r < kTileRows; r++)
+          for (int q = 0; q < kTileCols; q++) {
+            const int c = base + r * P + q;
+            if (!(type[c] & kExists)) continue;
+            any = true;
+            for (size_t j = 0; j < A.size() && full; j++)
+              if (!(type[c + A[j] * P + B[j]] & kExists)) full = false;
+          }
+        if (any) tiles.push_back(DenseTile{base, k, full ? 1 : 0, 0});
+      }
+    for (int a = h->abc_begin[k]; a < h->abc_begin[k] + round_up(h->abc_count[k], kNodeBlock); a++) {
+      H.inst[a] = k;
+      H.node[a] = c0;
+    }
+    pack_abc(p, h->opt, s, k, [&cell_of](int i) { return cell_of[i]; }, h->abc_begin[k], H, abc_of, type);
+    fill_params(h->params[k], p, h->opt, s);
+    InstParams &Pp = h->params[k];
+    Pp.node_begin = c0;
+    Pp.node_count = D.host_cells[k];
+    Pp.abc_begin = h->abc_begin[k];
+    Pp.abc_count = h->abc_count[k];
+    int nact = 0;
+    for (int i = 0; i < h->abc_count[k]; i++) nact += p.bctypes[2 * p.inf_nodes[i]] == 1;
+    Pp.n_active_abc = nact;
+    Pp.dense = 1;
+    Pp.pitch = P;
+    Pp.nrow = lat[k].NR;
+    Pp.ncol = lat[k].NC;
+    Pp.stencil = M;
+  }
+  // group tiles by stencil ratio
+  std::stable_sort(tiles.begin(), tiles.end(), [&](const DenseTile &x, const DenseTile &y) {
+    return lat[x.inst].M < lat[y.inst].M;
+  });
+  D.groups.clear();
+  for (int i = 0; i < (int)tiles.size(); i++) {
+    const int M = lat[tiles[i].inst].M;
+    if (D.groups.empty() || D.groups.back().m != M) D.groups.push_back(DenseGroup{M, i, 0});
+    D.groups.back().n_tiles++;
+  }
+  // upload
+  Geo &G = h->lg.geo;
+  Abc &Bb = h->lg.abc;
+  G.n_total = n;
+  G.ell_width = 0;
+  double2 *d_xy, *d_coef;
+  uint8_t *d_type;
+  int *d_abc_of, *d_blk;
+  double *d_m;
+  DenseTile *d_tiles;
+  int st;
+  if ((st = dev_upload(h, &d_xy, xy)) || (st = dev_upload(h, &d_coef, coef)) ||
+      (st = dev_upload(h, &d_type, type)) || (st = dev_upload(h, &d_abc_of, abc_of)) ||
+      (st = dev_upload(h, &d_blk, blk_inst)) || (st = dev_upload(h, &d_m, m)) ||
+      (st = dev_upload(h, &d_tiles, tiles)))
+    return st;
+  G.xy = d_xy; G.coef = d_coef; G.type = d_type; G.abc_of = d_abc_of; G.blk_inst = d_blk; G.m = d_m;
+  G.len = nullptr; G.nbr = nullptr;
+  D.tiles = d_tiles;
+  if ((st = upload_abc(h, H, total_abc))) return st;
+  (void)Bb;
+  std::map<int, int> done;
+  for (int k = 0; k < K; k++) {
+    if (done.count(lat[k].M)) continue;
+    done[lat[k].M] = 1;
+    LPS_CUDA_TRY(h, upload_dense_constants(lat[k].M, probs[k].dx, probs[k].dy, probs[k].delta, h->stream));
+  }
+  LPS_CUDA_TRY(h, dense_prepare_kernels());
+  h->lg.n_node_blocks = n / kNodeBlock;
   h->lg.n_abc_blocks = total_abc / kAbcWarpsPerBlock;
   h->lg.n_inst = K;
   h->lg.theta_method = h->opt.theta_method;
@@ -564,7 +803,7 @@ const char *lps_last_error(const lps_handle *h) {
 int lps_create(const lps_problem *problems, int n_instances, const lps_options *opt, lps_handle **out) {
   g_create_error.clear();
   if (!out || !problems || n_instances <= 0 || n_instances > kMaxInstances) {
-    g_create_error = "lps_create: bad arguments (need 1..256 instances and an output pointer)";
+    g_create_error = "lps_create: bad arguments (need 1..128 instances and an output pointer)";
     return LPS_ERR_INVALID_ARG;
   }
   *out = nullptr;
@@ -633,23 +872,16 @@ int lps_create(const lps_problem *problems, int n_instances, const lps_options *
   }
   // path choice: dense when every instance maps onto a lattice
   int s = LPS_OK;
-  bool dense_ok = o.path != LPS_PATH_CSR && dense_supported(problems, K, h->setup, o);
+  std::vector<Lattice> lat;
+  const bool dense_ok = o.path != LPS_PATH_CSR && dense_possible(problems, K, h->setup, lat);
   if (o.path == LPS_PATH_DENSE && !dense_ok) {
-    h->err = "lps_create: dense path requested but an instance is not a lattice";
+    h->err = "lps_create: dense path requested but an instance is not an exact dx = dy lattice "
+             "with delta/dx in {2,3,4,5,6,8} and no prenotch";
     return fail(LPS_ERR_UNSUPPORTED);
   }
   if (dense_ok) {
     h->path = LPS_PATH_DENSE;
-    s = build_dense(h->dg, h->lg, problems, K, h->setup, o, h->params, h->node_begin, h->node_count,
-                    h->abc_begin, h->abc_count, h->n_total, h->n_abc_total, h->err,
-                    [h](void **p, size_t bytes) {
-                      cudaError_t e = cudaMalloc(p, bytes);
-                      if (e == cudaSuccess) {
-                        h->allocs.push_back(*p);
-                        h->device_bytes += (int64_t)bytes;
-                      }
-                      return e;
-                    });
+    s = build_dense(h, problems, lat);
   } else {
     h->path = LPS_PATH_CSR;
     s = build_csr(h, problems);

@@ -22,7 +22,7 @@
 
 namespace lps {
 
-constexpr int kMaxInstances = 256;   // entries of the __constant__ table (176 B each)
+constexpr int kMaxInstances = 128;   // entries of the __constant__ table (176 B each)
 constexpr int kNodeBlock = 256;      // threads per node-kernel block
 constexpr int kAbcWarpsPerBlock = 8; // warps per ABC block (one ABC node each)
 

@@ -82,7 +82,9 @@ def test_oracle_parity_generated(m, path):
         assert rel_l2(st[k], r[k]) <= DERIVED_TOL, k
     dE = r["diag"]["dE_rel"]
     assert np.max(np.abs(d["dE_rel"] - dE)) <= DE_TOL
-    np.testing.assert_array_equal(d["max_u_node"], r["diag"]["max_u_node"])
+    # the argmax node of a radial pulse is a near-tie that round-off may flip;
+    # compare the maximum itself
+    np.testing.assert_allclose(d["max_u"], r["diag"]["max_u"], rtol=1e-12, atol=0)
 
 
 @pytest.mark.parametrize("path", PATHS)
