@@ -52,7 +52,8 @@ struct lps_handle {
   std::vector<int> local_of_global;  // for dense: cell -> local node index
 
   // state
-  double2 *U[3] = {}, *V[3] = {}, *A[2] = {}, *VH = nullptr, *S = nullptr;
+  double2 *U[kUring] = {}, *V[3] = {}, *A[2] = {}, *VH = nullptr, *S = nullptr;
+  int ring_u = 3;             // displacement ring depth: 3 (CSR path) or 4 (dense path)
   double *TH[3] = {};
   double2 *U0 = nullptr, *V0 = nullptr;
   // diagnostics
@@ -65,7 +66,7 @@ struct lps_handle {
 
   int64_t step = 0;          // steps taken since reset
   int64_t launches = 0;
-  std::map<int, cudaGraphExec_t> graphs;  // key: 6-bit diag mask
+  std::map<int, cudaGraphExec_t> graphs;  // key: diag mask of the captured steps
   std::map<int, int> graph_kernels;
 };
 
@@ -430,31 +431,37 @@ int build_dense(lps_handle *h, const lps_problem *probs, const std::vector<Latti
   D.host_node_of_cell_v.assign(K, {});
   D.host_cells.assign(K, 0);
   D.host_cell_begin.assign(K, 0);
-  std::vector<int> pitch(K), rows(K), cols(K);
-  long total = 0;
+  // one pitch for the batch (multiple of 32 cells, at least one tile width of
+  // slack past the padded lattice so the 48-byte type boxes stay in the row)
+  int P = 0;
+  for (int k = 0; k < K; k++)
+    P = std::max(P, round_up(round_up(lat[k].NC, kTileCols) + 2 * lat[k].M, 32));
+  std::vector<int> rows(K), cols(K), row_begin(K);
+  long total_rows = 0;
   int total_abc = 0;
   for (int k = 0; k < K; k++) {
     const int M = lat[k].M;
-    const int NRt = round_up(lat[k].NR, kTileRows), NCt = round_up(lat[k].NC, kTileCols);
-    rows[k] = NRt + 2 * M;
-    cols[k] = NCt;
-    pitch[k] = round_up(NCt + 2 * M, 8);
-    const long cells = (long)round_up(rows[k] * pitch[k], kNodeBlock);
-    D.host_cell_begin[k] = (int)total;
-    D.host_cells[k] = (int)cells;
-    h->node_begin[k] = (int)total;
+    const int NRt = round_up(lat[k].NR, kTileRows);
+    rows[k] = round_up(NRt + 2 * M, 8);  // 8 rows x 32k cells: bands start on 256-cell blocks
+    cols[k] = round_up(lat[k].NC, kTileCols);
+    row_begin[k] = (int)total_rows;
+    total_rows += rows[k];
+    D.host_cell_begin[k] = row_begin[k] * P;
+    D.host_cells[k] = rows[k] * P;
+    h->node_begin[k] = D.host_cell_begin[k];
     h->node_count[k] = probs[k].n_nodes;
-    total += cells;
     const bool abc_on = h->opt.abcs_step != -1 && probs[k].n_abc > 0;
     h->abc_begin[k] = total_abc;
     h->abc_count[k] = abc_on ? probs[k].n_abc : 0;
     total_abc += round_up(h->abc_count[k], kNodeBlock);
   }
-  if (total > 2000000000L) {
+  if (total_rows * (long)P > 2000000000L) {
     h->err = "lps_create: dense layout larger than 2^31 cells";
     return LPS_ERR_UNSUPPORTED;
   }
-  const int n = (int)total;
+  const int n = (int)(total_rows * P);
+  D.pitch = P;
+  D.total_rows = (int)total_rows;
   h->n_total = n;
   h->n_abc_total = total_abc;
   std::vector<double2> xy(n, make_double2(0, 0)), coef(n, make_double2(0, -1));
@@ -466,11 +473,10 @@ int build_dense(lps_handle *h, const lps_problem *probs, const std::vector<Latti
   H.cl_off.assign(total_abc, 0); H.cl_len.assign(total_abc, 0);
   H.idw_off.assign(total_abc, 0); H.idw_len.assign(total_abc, 0);
   H.writes.assign(total_abc, 0); H.active.assign(total_abc, 0);
-  std::vector<DenseTile> tiles;
   for (int k = 0; k < K; k++) {
     const lps_problem &p = probs[k];
     const InstanceSetup &s = h->setup[k];
-    const int M = lat[k].M, P = pitch[k], c0 = D.host_cell_begin[k];
+    const int M = lat[k].M, c0 = D.host_cell_begin[k];
     for (int b = c0 / kNodeBlock; b < (c0 + D.host_cells[k]) / kNodeBlock; b++) blk_inst[b] = k;
     auto &cell_of = D.host_cell_of_node[k];
     auto &node_of = D.host_node_of_cell_v[k];
@@ -485,24 +491,6 @@ int build_dense(lps_handle *h, const lps_problem *probs, const std::vector<Latti
       m[c] = s.m[i];
       if (s.m[i] > 0.0) coef[c] = make_double2(2.0 * (s.lam - s.mu) / s.m[i], 8.0 * s.mu / s.m[i]);
     }
-    // tiles: owned rows [r0, r0 + 16), columns [c, c + 32) of the lattice
-    std::vector<int> A, B;
-    dense_offsets(M, A, B);
-    const int NRt = rows[k] - 2 * M;
-    for (int r0 = 0; r0 < NRt; r0 += kTileRows)
-      for (int q0 = 0; q0 < cols[k]; q0 += kTileCols) {
-        const int base = c0 + (r0 + M) * P + (q0 + M);
-        bool any = false, full = true;
-        for (int r = 0; r < kTileRows; r++)
-          for (int q = 0; q < kTileCols; q++) {
-            const int c = base + r * P + q;
-            if (!(type[c] & kExists)) continue;
-            any = true;
-            for (size_t j = 0; j < A.size() && full; j++)
-              if (!(type[c + A[j] * P + B[j]] & kExists)) full = false;
-          }
-        if (any) tiles.push_back(DenseTile{base, k, full ? 1 : 0, 0});
-      }
     for (int a = h->abc_begin[k]; a < h->abc_begin[k] + round_up(h->abc_count[k], kNodeBlock); a++) {
       H.inst[a] = k;
       H.node[a] = c0;
@@ -523,19 +511,53 @@ int build_dense(lps_handle *h, const lps_problem *probs, const std::vector<Latti
     Pp.ncol = lat[k].NC;
     Pp.stencil = M;
   }
-  // group tiles by stencil ratio
+  // tiles: owned lattice rows [r0, r0+16) x columns [q0, q0+32); the staged
+  // region starts m rows and m columns earlier
+  std::vector<DenseTile> tiles;
+  for (int k = 0; k < K; k++) {
+    const int M = lat[k].M;
+    std::vector<int> A, B;
+    dense_offsets(M, A, B);
+    const int NRt = round_up(lat[k].NR, kTileRows);
+    for (int r0 = 0; r0 < NRt; r0 += kTileRows)
+      for (int q0 = 0; q0 < cols[k]; q0 += kTileCols) {
+        const int region_row = row_begin[k] + r0, region_col = q0;
+        const long first = (long)(region_row + M) * P + region_col + M;
+        bool any = false, full = true, abc = false;
+        for (int r = 0; r < kTileRows; r++)
+          for (int q = 0; q < kTileCols; q++) {
+            const long c = first + (long)r * P + q;
+            if (!(type[c] & kExists)) continue;
+            any = true;
+            for (size_t j = 0; j < A.size() && full; j++)
+              if (!(type[c + (long)A[j] * P + B[j]] & kExists)) full = false;
+          }
+        for (int r = 0; r < kTileRows + 2 * M && !abc; r++)
+          for (int q = 0; q < kTileCols + 2 * M; q++)
+            if (type[(long)(region_row + r) * P + region_col + q] & kActiveAbc) {
+              abc = true;
+              break;
+            }
+        if (any)
+          tiles.push_back(DenseTile{region_row, region_col, k, (full ? kTileFull : 0) | (abc ? kTileAbc : 0)});
+      }
+  }
   std::stable_sort(tiles.begin(), tiles.end(), [&](const DenseTile &x, const DenseTile &y) {
     return lat[x.inst].M < lat[y.inst].M;
   });
   D.groups.clear();
   for (int i = 0; i < (int)tiles.size(); i++) {
     const int M = lat[tiles[i].inst].M;
-    if (D.groups.empty() || D.groups.back().m != M) D.groups.push_back(DenseGroup{M, i, 0});
+    if (D.groups.empty() || D.groups.back().m != M) {
+      D.groups.emplace_back();
+      D.groups.back().m = M;
+      D.groups.back().tile_begin = i;
+      D.groups.back().n_tiles = 0;
+    }
     D.groups.back().n_tiles++;
   }
   // upload
   Geo &G = h->lg.geo;
-  Abc &Bb = h->lg.abc;
   G.n_total = n;
   G.ell_width = 0;
   double2 *d_xy, *d_coef;
@@ -553,14 +575,13 @@ int build_dense(lps_handle *h, const lps_problem *probs, const std::vector<Latti
   G.len = nullptr; G.nbr = nullptr;
   D.tiles = d_tiles;
   if ((st = upload_abc(h, H, total_abc))) return st;
-  (void)Bb;
   std::map<int, int> done;
   for (int k = 0; k < K; k++) {
     if (done.count(lat[k].M)) continue;
     done[lat[k].M] = 1;
     LPS_CUDA_TRY(h, upload_dense_constants(lat[k].M, probs[k].dx, probs[k].dy, probs[k].delta, h->stream));
   }
-  LPS_CUDA_TRY(h, dense_prepare_kernels());
+  LPS_CUDA_TRY(h, dense_prepare(D));
   h->lg.n_node_blocks = n / kNodeBlock;
   h->lg.n_abc_blocks = total_abc / kAbcWarpsPerBlock;
   h->lg.n_inst = K;
@@ -569,15 +590,40 @@ int build_dense(lps_handle *h, const lps_problem *probs, const std::vector<Latti
   return LPS_OK;
 }
 
+// Dense path, after the state buffers exist: TMA descriptors, the forked
+// stream for the absorbing-boundary kernels and the device error flag.
+int finish_dense(lps_handle *h) {
+  DenseGeo &D = h->dg;
+  const double2 *coef = h->lg.geo.coef;
+  const uint8_t *type = h->lg.geo.type;
+  for (auto &gr : D.groups) {
+    const int s = dense_encode_maps(gr, D.pitch, D.total_rows, h->U, h->TH, coef, type, h->err);
+    if (s) return s;
+  }
+  LPS_CUDA_TRY(h, cudaStreamCreateWithFlags(&D.side, cudaStreamNonBlocking));
+  for (int i = 0; i < 2; i++) {
+    LPS_CUDA_TRY(h, cudaEventCreateWithFlags(&D.ev_fork[i], cudaEventDisableTiming));
+    LPS_CUDA_TRY(h, cudaEventCreateWithFlags(&D.ev_join[i], cudaEventDisableTiming));
+  }
+  int s;
+  if ((s = dev_alloc(h, &D.d_err, 1))) return s;
+  LPS_CUDA_TRY(h, cudaMemset(D.d_err, 0, sizeof(int)));
+  return LPS_OK;
+}
+
 // ---------------------------------------------------------------------------
 // Ring indices of step s (1-based) whose current level is n = s - 1.
 StepPtrs step_ptrs(lps_handle *h, int64_t n) {
   StepPtrs p;
+  const int R = h->ring_u;
   const int u0 = (int)(n % 3), u1 = (int)((n + 1) % 3), um = (int)((n + 2) % 3);
   const int a0 = (int)(n % 2), a1 = (int)((n + 1) % 2);
-  p.u_n = h->U[u0];
-  p.u_nm1 = h->U[um];
-  p.u_np1 = h->U[u1];
+  p.u_n = h->U[n % R];
+  p.u_nm1 = h->U[(n + R - 1) % R];
+  p.u_np1 = h->U[(n + 1) % R];
+  p.u_np2 = h->U[(n + 2) % R];
+  p.th_ring = u1;
+  p.pad = 0;
   p.v_n = h->V[u0];
   p.v_nm1 = h->V[um];
   p.v_np1 = h->V[u1];
@@ -601,7 +647,7 @@ int enqueue_step(lps_handle *h, int64_t n, bool diag, const Mark *mark = nullptr
   };
   int k = 0;
   if (h->path == LPS_PATH_DENSE) {
-    k += enqueue_dense_step(h->dg, h->lg, p, h->d_step, st, mark);
+    k += enqueue_dense_step(h->dg, h->lg, p, h->d_step, st, mark, (int)((n + 1) % h->ring_u));
   } else {
     launch_predict_csr(h->lg, p, st);
     M("predict_csr");
@@ -653,6 +699,22 @@ int drain_log(lps_handle *h) {
   return LPS_OK;
 }
 
+// Steps per captured graph: the least common multiple of the ring depths, so
+// a graph that starts on a multiple of it finds every buffer where it
+// captured it.
+int graph_period(const lps_handle *h) { return h->ring_u == 4 ? 12 : 6; }
+
+int check_device_error(lps_handle *h) {
+  if (h->path != LPS_PATH_DENSE || !h->dg.d_err) return LPS_OK;
+  int e = 0;
+  LPS_CUDA_TRY(h, cudaMemcpy(&e, h->dg.d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (e) {
+    h->err = "a device-side wait on a tile copy timed out";
+    return LPS_ERR_CUDA;
+  }
+  return LPS_OK;
+}
+
 int get_graph(lps_handle *h, int mask, cudaGraphExec_t *out) {
   auto it = h->graphs.find(mask);
   if (it != h->graphs.end()) {
@@ -662,7 +724,7 @@ int get_graph(lps_handle *h, int mask, cudaGraphExec_t *out) {
   cudaGraph_t g;
   LPS_CUDA_TRY(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
   int kernels = 0;
-  for (int r = 0; r < 6; r++) kernels += enqueue_step(h, r, (mask >> r) & 1);
+  for (int r = 0; r < graph_period(h); r++) kernels += enqueue_step(h, r, (mask >> r) & 1);
   LPS_CUDA_TRY(h, cudaStreamEndCapture(h->stream, &g));
   cudaGraphExec_t ex;
   cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
@@ -698,8 +760,8 @@ __global__ void k_reset_abc(Abc ab, const double2 *u0, double2 *s) {
 int do_reset(lps_handle *h) {
   cudaStream_t st = h->stream;
   const int n = h->n_total;
-  k_reset_state<<<(n + 255) / 256, 256, 0, st>>>(n, h->U0, h->V0, h->U[0], h->U[2], h->V[0], h->V[2],
-                                                  h->A[0], h->TH[2]);
+  k_reset_state<<<(n + 255) / 256, 256, 0, st>>>(n, h->U0, h->V0, h->U[0], h->U[h->ring_u - 1], h->V[0],
+                                                  h->V[2], h->A[0], h->TH[2]);
   LPS_CUDA_TRY(h, cudaMemsetAsync(h->TH[0], 0, sizeof(double) * n, st));
   if (h->n_abc_total > 0)
     k_reset_abc<<<(h->n_abc_total + 255) / 256, 256, 0, st>>>(h->lg.abc, h->U0, h->S);
@@ -710,6 +772,9 @@ int do_reset(lps_handle *h) {
     else
       launch_theta_csr(h->lg, h->U[0], h->TH[0], nullptr, nullptr, false, st);
   }
+  // dense path: the force pass predicts the next level, so level 1 is
+  // predicted here (src/main.cpp:727 with a^0 = 0)
+  if (h->path == LPS_PATH_DENSE) launch_dense_reset_predict(h->lg, h->U0, h->V0, h->U[1], h->VH, st);
   LPS_CUDA_TRY(h, cudaMemsetAsync(h->d_step, 0, sizeof(int), st));
   LPS_CUDA_TRY(h, cudaMemsetAsync(h->log_count, 0, sizeof(int) * h->n_inst, st));
   LPS_CUDA_TRY(h, cudaGetLastError());
@@ -725,10 +790,12 @@ int do_reset(lps_handle *h) {
 int alloc_state(lps_handle *h) {
   const int n = h->n_total;
   int s;
-  for (int r = 0; r < 3; r++) {
-    if ((s = dev_alloc(h, &h->U[r], n)) || (s = dev_alloc(h, &h->V[r], n)) || (s = dev_alloc(h, &h->TH[r], n)))
-      return s;
+  for (int r = 0; r < h->ring_u; r++) {
+    if ((s = dev_alloc(h, &h->U[r], n))) return s;
     LPS_CUDA_TRY(h, cudaMemset(h->U[r], 0, sizeof(double2) * n));
+  }
+  for (int r = 0; r < 3; r++) {
+    if ((s = dev_alloc(h, &h->V[r], n)) || (s = dev_alloc(h, &h->TH[r], n))) return s;
     LPS_CUDA_TRY(h, cudaMemset(h->V[r], 0, sizeof(double2) * n));
     LPS_CUDA_TRY(h, cudaMemset(h->TH[r], 0, sizeof(double) * n));
   }
@@ -771,6 +838,13 @@ void destroy_all(lps_handle *h) {
   h->graphs.clear();
   for (void *p : h->allocs) cudaFree(p);
   h->allocs.clear();
+  for (int i = 0; i < 2; i++) {
+    if (h->dg.ev_fork[i]) cudaEventDestroy(h->dg.ev_fork[i]);
+    if (h->dg.ev_join[i]) cudaEventDestroy(h->dg.ev_join[i]);
+    h->dg.ev_fork[i] = h->dg.ev_join[i] = nullptr;
+  }
+  if (h->dg.side) cudaStreamDestroy(h->dg.side);
+  h->dg.side = nullptr;
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
   h->stream = nullptr;
 }
@@ -881,6 +955,7 @@ int lps_create(const lps_problem *problems, int n_instances, const lps_options *
   }
   if (dense_ok) {
     h->path = LPS_PATH_DENSE;
+    h->ring_u = kUring;
     s = build_dense(h, problems, lat);
   } else {
     h->path = LPS_PATH_CSR;
@@ -893,6 +968,7 @@ int lps_create(const lps_problem *problems, int n_instances, const lps_options *
     return fail(LPS_ERR_CUDA);
   }
   if ((s = alloc_state(h))) return fail(s);
+  if (h->path == LPS_PATH_DENSE && (s = finish_dense(h))) return fail(s);
   // initial conditions
   {
     std::vector<double2> u0(h->n_total, make_double2(0, 0)), v0(h->n_total, make_double2(0, 0));
@@ -951,7 +1027,8 @@ int lps_step(lps_handle *h, int n_steps, int diag_every) {
   int remaining = n_steps;
   while (remaining > 0) {
     // records this chunk adds per instance must fit in the device log
-    const int chunk = (h->step % 6 == 0 && remaining >= 6 && h->opt.use_graphs) ? 6 : 1;
+    const int G = graph_period(h);
+    const int chunk = (h->step % G == 0 && remaining >= G && h->opt.use_graphs) ? G : 1;
     int new_rec = 0, mask = 0;
     for (int r = 0; r < chunk; r++) {
       const int64_t s = h->step + 1 + r;
@@ -964,7 +1041,7 @@ int lps_step(lps_handle *h, int n_steps, int diag_every) {
       int st = drain_log(h);
       if (st) return st;
     }
-    if (chunk == 6) {
+    if (chunk > 1) {
       cudaGraphExec_t ex;
       int st = get_graph(h, mask, &ex);
       if (st) return st;
@@ -986,6 +1063,7 @@ int lps_read_diag(lps_handle *h, int instance, lps_diag *out, int max_records, i
   int st = drain_log(h);
   if (st) return st;
   LPS_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  if ((st = check_device_error(h))) return st;
   std::vector<DiagRecord> &v = h->drained[instance];
   const int n = std::min((int)v.size(), std::max(max_records, 0));
   int status = LPS_OK;
@@ -1018,14 +1096,13 @@ int lps_read_diag(lps_handle *h, int instance, lps_diag *out, int max_records, i
 int lps_download(lps_handle *h, int instance, double *u, double *v, double *a, double *theta, double *m) {
   if (!h || instance < 0 || instance >= h->n_inst) return LPS_ERR_INVALID_ARG;
   const int64_t n = h->step;
-  const StepPtrs p = step_ptrs(h, n > 0 ? n - 1 : 0);
   // the newest level: after step n the current level is n
-  const int cur = (int)(n % 3), cura = (int)(n % 2);
+  const int cur = (int)(n % h->ring_u), cur3 = (int)(n % 3), cura = (int)(n % 2);
   if (h->opt.abcs_step != -1 && h->lg.abc.n_abc > 0) launch_merge_abc(h->lg, h->U[cur], h->S, h->stream);
-  (void)p;
   LPS_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  if (int e = check_device_error(h)) return e;
   const int nn = h->node_count[instance];
-  const int g0 = h->path == LPS_PATH_DENSE ? h->node_begin[instance] : h->node_begin[instance];
+  const int g0 = h->node_begin[instance];
   const int span = h->path == LPS_PATH_DENSE ? h->dg.host_cells[instance] : nn;
   std::vector<double2> b2(span);
   std::vector<double> b1(span);
@@ -1046,8 +1123,8 @@ int lps_download(lps_handle *h, int instance, double *u, double *v, double *a, d
     return LPS_OK;
   };
   int s;
-  if ((s = get2(h->U[cur], u)) || (s = get2(h->V[cur], v)) || (s = get2(h->A[cura], a)) ||
-      (s = get1(h->TH[cur], theta)))
+  if ((s = get2(h->U[cur], u)) || (s = get2(h->V[cur3], v)) || (s = get2(h->A[cura], a)) ||
+      (s = get1(h->TH[cur3], theta)))
     return s;
   if (m) {
     const InstanceSetup &su = h->setup[instance];
@@ -1059,6 +1136,7 @@ int lps_download(lps_handle *h, int instance, double *u, double *v, double *a, d
 int lps_synchronize(lps_handle *h) {
   if (!h) return LPS_ERR_INVALID_ARG;
   LPS_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  if (int e = check_device_error(h)) return e;
   return LPS_OK;
 }
 

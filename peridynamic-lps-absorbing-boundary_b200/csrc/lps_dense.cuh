@@ -2,15 +2,19 @@
 //
 // Every instance whose nodes sit exactly on a dx = dy lattice with
 // delta = m dx (m in kDenseM) is stored as a padded 2-D grid of cells:
-// row = x index, column = y index (so cell order follows the
-// preprocessor's node order, x outer / y inner, preprocessor/main.cpp:851),
-// column pitch a multiple of 8 cells (128-byte rows of double2), m cells of
-// padding on every side plus the round-up to whole tiles.  Empty cells carry
-// type 0.  The horizon of a cell is the fixed offset set
+// row = x index, column = y index (cell order follows the preprocessor's
+// node order, x outer / y inner, preprocessor/main.cpp:851), m cells of
+// padding on every side plus the round-up to whole tiles.  All instances of a
+// batch share one column pitch (a multiple of 32 cells), so each state buffer
+// is one 2-D tensor [rows][pitch] that one TMA descriptor covers; instance k
+// owns a band of rows starting at a multiple of 8.  Empty cells carry type 0.
+// The horizon of a cell is the fixed offset set
 // {(a, b) != 0 : a^2 + b^2 <= m^2 + m} -- exactly the nodes the reference's
 // search radius delta + dx/2 + 1e-5 (src/main.cpp:352) admits on such a
 // lattice -- restricted to existing cells.
 #pragma once
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <string>
@@ -24,24 +28,47 @@ namespace lps {
 
 constexpr int kTileRows = 16;   // owned cells per tile: 16 rows x 32 columns
 constexpr int kTileCols = 32;
+constexpr int kCellsPerThread = 4;                                // consecutive rows
+constexpr int kTileThreads = kTileRows * kTileCols / kCellsPerThread;  // 128
 constexpr int kDenseM[] = {2, 3, 4, 5, 6, 8};
+constexpr int kUring = 4;       // displacement ring depth of the dense path
+
+// tile flags
+constexpr int kTileFull = 1;    // every neighbour of every owned node exists
+constexpr int kTileAbc = 2;     // the staged region holds an active ABC node
 
 struct DenseTile {
-  int base;   // global cell index of the tile's first owned cell
+  int row;    // global row of the staged region's first row
+  int col;    // column of the staged region's first column
   int inst;   // instance id
-  int full;   // 1: every neighbour of every owned node exists (no masking)
-  int pad;
+  int flags;
+};
+
+// TMA descriptors of one stencil ratio (box sizes depend on m).
+struct DenseMaps {
+  CUtensorMap u[kUring];  // displacement ring, double2 viewed as 2 x f64
+  CUtensorMap th[3];      // theta ring
+  CUtensorMap coef;       // (2(l-m)/m_i, 8 mu/m_i)
+  CUtensorMap type;       // u8 node type
 };
 
 struct DenseGroup {
   int m;            // stencil ratio of the tiles in this group
   int tile_begin;   // first tile in the device tile list
   int n_tiles;
+  int grid_theta;   // persistent grid sizes
+  int grid_force;
+  DenseMaps maps;
 };
 
 struct DenseGeo {
   const DenseTile *tiles = nullptr;            // device
   std::vector<DenseGroup> groups;
+  int pitch = 0;
+  int total_rows = 0;
+  cudaStream_t side = nullptr;                 // forked stream for the ABC kernels
+  cudaEvent_t ev_fork[2] = {nullptr, nullptr}, ev_join[2] = {nullptr, nullptr};
+  int *d_err = nullptr;                        // device wait-timeout flag
   std::vector<std::vector<int>> host_cell_of_node;  // per instance: local node -> global cell
   std::vector<int> host_cells;                      // per instance: cell span
   std::vector<int> host_cell_begin;                 // per instance: first cell
@@ -59,14 +86,22 @@ void dense_offsets(int m, std::vector<int> &a, std::vector<int> &b);
 // Per-offset FP64 constants of ratio m for lattice spacing dx (= dy) and
 // horizon delta, into __constant__ memory.
 cudaError_t upload_dense_constants(int m, double dx, double dy, double delta, cudaStream_t st);
+// Encodes the TMA descriptors of group g over the given buffers.
+int dense_encode_maps(DenseGroup &g, int pitch, int total_rows, double2 *const *U, double *const *TH,
+                      const double2 *coef, const uint8_t *type, std::string &err);
+// Sets shared-memory limits and the persistent grid sizes of each group.
+cudaError_t dense_prepare(DenseGeo &dg);
 
+// One time step: theta tiles || G_theta, [IDW], force tiles || G_u/G_v.
 int enqueue_dense_step(const DenseGeo &dg, const LaunchGeo &lg, const StepPtrs &p, int *d_step,
-                       cudaStream_t st, const Mark *mark);
+                       cudaStream_t st, const Mark *mark, int ring_u);
+// Reset helpers: predicted u^1 and vh for every cell from u^0, v^0.
+void launch_dense_reset_predict(const LaunchGeo &lg, const double2 *u0, const double2 *v0, double2 *u1,
+                                double2 *vh, cudaStream_t st);
 void launch_theta_dense_init(const DenseGeo &dg, const LaunchGeo &lg, const double2 *u, double *theta,
                              cudaStream_t st);
 void launch_diag_dense(const DenseGeo &dg, const LaunchGeo &lg, const double2 *u, const double2 *v,
                        const double2 *a, const double *theta, DiagPartial *partials, DiagRecord *log,
                        int *log_count, int log_capacity, const int *d_step, cudaStream_t st);
-cudaError_t dense_prepare_kernels();
 
 }  // namespace lps

@@ -67,6 +67,9 @@ struct StepPtrs {
   const double *th_n, *th_nm1;
   double *th_np1;
   double2 *s_abc;          // G_u result u^{n+1} at ABC nodes, merged next step
+  double2 *u_np2;          // dense path: predicted u^{n+2}, written by the force pass
+  int th_ring;             // ring index of th_np1
+  int pad;
 };
 
 // Geometry + static per-node data.

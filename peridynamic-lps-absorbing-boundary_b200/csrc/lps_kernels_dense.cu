@@ -1,16 +1,21 @@
 // lps_kernels_dense.cu -- masked dense-grid stencil kernels, FP64, sm_100a.
 //
-// One time step is two launches per stencil group:
-//   k_theta_dense<M>: predictor (src/main.cpp:725-728) over a tile plus its
-//     m-cell halo staged in shared memory, then the dilatation (:736-761) of
-//     the owned cells; extra blocks apply G_theta at ABC nodes (:792-812).
-//   k_force_dense<M>: the force (:821-874) over a tile plus halo of predicted
-//     displacements and theta coefficients, with the corrector (:922-925)
-//     fused; extra blocks apply G_u / G_v (:883-916, :933-974).
-// The offsets (a, b) are compile-time constants of M, the per-offset FP64
-// weights live in __constant__ memory, so each bond is a handful of FP64
-// FMAs on shared-memory operands.
+// One time step is two persistent tile kernels, each with a concurrent
+// absorbing-boundary kernel on a forked stream:
+//   k_theta_tma<M>  || k_abc_theta   dilatation (src/main.cpp:736-761) of the
+//                                    predicted displacements || G_theta (:792-812)
+//   k_force_tma<M>  || k_abc_uv      force (:821-874), corrector (:922-925) and
+//                                    the next step's predictor (:725-728)
+//                                    || G_u, G_v (:883-916, :933-974)
+// Tile kernels stage a 16 x 32 tile plus its m-cell halo with TMA
+// (cp.async.bulk.tensor) into one of two shared-memory buffers while the
+// other buffer is being computed; every wait on the transaction barrier is
+// bounded and reports a timeout through an error flag.  Each thread owns 4
+// consecutive rows of one column and walks the stencil column by column,
+// pairing offset (a, b) with (-a, -b), so every staged value it loads feeds
+// several bonds.
 #include <cmath>
+#include <cstdio>
 
 #include "lps_abc.cuh"
 #include "lps_common.cuh"
@@ -19,13 +24,30 @@
 namespace lps {
 
 // ---------------------------------------------------------------------------
-// compile-time stencils: {(a, b) != 0 : a^2 + b^2 <= M^2 + M}
+// compile-time stencils: {(a, b) != 0 : a^2 + b^2 <= M^2 + M}, enumerated
+// a-major from (-M, -M); offset j and N-1-j are negatives of each other.
 __host__ __device__ constexpr int sten_count(int M) {
   int n = 0;
   for (int a = -M; a <= M; a++)
     for (int b = -M; b <= M; b++)
       if ((a != 0 || b != 0) && a * a + b * b <= M * M + M) n++;
   return n;
+}
+__host__ __device__ constexpr int sten_index(int M, int a0, int b0) {
+  int n = 0;
+  for (int a = -M; a <= M; a++)
+    for (int b = -M; b <= M; b++)
+      if ((a != 0 || b != 0) && a * a + b * b <= M * M + M) {
+        if (a == a0 && b == b0) return n;
+        n++;
+      }
+  return -1;
+}
+// largest |a| with a^2 + b^2 <= M^2 + M
+__host__ __device__ constexpr int amax(int M, int b) {
+  int A = 0;
+  while ((A + 1) * (A + 1) + b * b <= M * M + M) A++;
+  return A;
 }
 
 template <int M>
@@ -81,16 +103,21 @@ static void offsets_of(std::vector<int> &a, std::vector<int> &b) {
   b.assign(s.b, s.b + Sten<M>::N);
 }
 
-void dense_offsets(int m, std::vector<int> &a, std::vector<int> &b) {
-  switch (m) {
-    case 2: offsets_of<2>(a, b); break;
-    case 3: offsets_of<3>(a, b); break;
-    case 4: offsets_of<4>(a, b); break;
-    case 5: offsets_of<5>(a, b); break;
-    case 6: offsets_of<6>(a, b); break;
-    case 8: offsets_of<8>(a, b); break;
-    default: a.clear(); b.clear();
+#define LPS_DISPATCH_M(m, FN, ...)      \
+  switch (m) {                          \
+    case 2: FN<2>(__VA_ARGS__); break;  \
+    case 3: FN<3>(__VA_ARGS__); break;  \
+    case 4: FN<4>(__VA_ARGS__); break;  \
+    case 5: FN<5>(__VA_ARGS__); break;  \
+    case 6: FN<6>(__VA_ARGS__); break;  \
+    case 8: FN<8>(__VA_ARGS__); break;  \
+    default: break;                     \
   }
+
+void dense_offsets(int m, std::vector<int> &a, std::vector<int> &b) {
+  a.clear();
+  b.clear();
+  LPS_DISPATCH_M(m, offsets_of, a, b);
 }
 
 cudaError_t upload_dense_constants(int m, double dx, double dy, double delta, cudaStream_t st) {
@@ -120,191 +147,421 @@ cudaError_t upload_dense_constants(int m, double dx, double dy, double delta, cu
 }
 
 // ---------------------------------------------------------------------------
+// staged region geometry
 template <int M>
 struct Region {
   static constexpr int RR = kTileRows + 2 * M;   // staged rows
-  static constexpr int RC = kTileCols + 2 * M;   // staged columns
+  static constexpr int RC = kTileCols + 2 * M;   // staged columns (f64 boxes)
+  static constexpr int RT = 48;                  // staged columns of the u8 box (x16 bytes)
   static constexpr int CELLS = RR * RC;
+  static_assert(RC <= RT, "type box narrower than the region");
+  static constexpr int U_BYTES = CELLS * 16;
+  static constexpr int TH_BYTES = CELLS * 8;
+  static constexpr int CO_BYTES = CELLS * 16;
+  static constexpr int TY_BYTES = RR * RT;
+  static constexpr int align128(int x) { return (x + 127) / 128 * 128; }
+  // every TMA destination starts on a 128-byte boundary
+  // theta stage: u | type
+  static constexpr int T_TY = align128(U_BYTES);
+  static constexpr int THETA_STAGE = align128(T_TY + TY_BYTES);
+  static constexpr int THETA_TX = U_BYTES + TY_BYTES;
+  // force stage: u | th | coef | type
+  static constexpr int F_TH = align128(U_BYTES);
+  static constexpr int F_CO = align128(F_TH + TH_BYTES);
+  static constexpr int F_TY = align128(F_CO + CO_BYTES);
+  static constexpr int FORCE_STAGE = align128(F_TY + TY_BYTES);
+  static constexpr int FORCE_TX = U_BYTES + TH_BYTES + CO_BYTES + TY_BYTES;
+  static constexpr int THETA_SMEM = 2 * THETA_STAGE + 64;
+  static constexpr int FORCE_SMEM = 2 * FORCE_STAGE + 64;
 };
 
-template <int M>
-constexpr size_t theta_smem() {
-  return Region<M>::CELLS * (sizeof(double2) + 1);
+// ---- TMA / mbarrier primitives (inline PTX) --------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
-template <int M>
-constexpr size_t force_smem() {
-  return Region<M>::CELLS * (sizeof(double2) + 2 * sizeof(double) + 1);
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
-// Predictor + dilatation.  Block = one tile (256 threads: 8 warps x 32
-// columns, two owned rows per thread).
-template <int M>
-__global__ void __launch_bounds__(256)
-    k_theta_dense(Geo g, Abc ab, const DenseTile *__restrict__ tiles, StepPtrs p, int tile_begin,
-                  int n_tiles, int skip_abc) {
-  // blocks past the tiles exist only in the first group's launch
-  if ((int)blockIdx.x >= n_tiles) {
-    const int a = (blockIdx.x - n_tiles) * kAbcWarpsPerBlock + (threadIdx.x >> 5);
-    abc_theta_warp(ab, a, p.th_n, p.th_nm1, p.th_np1);
-    return;
+// Bounded wait on a transaction barrier: gives up after ~2 s (clock64) or
+// 2^26 polls, whichever comes first, and raises the error flag.
+constexpr int kErrWaitTimeout = 1;
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, int *err) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const long long t0 = clock64();
+  for (int it = 0; it < (1 << 26); it++) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (clock64() - t0 > 4000000000LL) break;
   }
+  atomicExch(err, kErrWaitTimeout);
+  return false;
+}
+
+// ---------------------------------------------------------------------------
+// Predictor + dilatation, persistent over tiles.
+template <int M>
+__device__ __forceinline__ void theta_tile_full(const double2 *__restrict__ su, int lane, int r0, double2 ui[4],
+                                                double s0[4], double s1[4]) {
   using R = Region<M>;
-  extern __shared__ __align__(16) unsigned char smem[];
-  double2 *su = reinterpret_cast<double2 *>(smem);
-  uint8_t *st = reinterpret_cast<uint8_t *>(su + R::CELLS);
-  const DenseTile t = tiles[tile_begin + blockIdx.x];
-  const InstParams &P = c_inst[t.inst];
-  const int pitch = P.pitch;
-  const double dt = P.dt, hdt = P.half_dt;
-  for (int q = threadIdx.x; q < R::CELLS; q += 256) {
-    const int rr = q / R::RC, cc = q - rr * R::RC;
-    const int cell = t.base + (rr - M) * pitch + (cc - M);
-    const uint8_t ty = g.type[cell];
-    double2 up = make_double2(0.0, 0.0);
-    if (ty & kExists) {
-      double2 u = p.u_n[cell];
-      if (ty & kActiveAbc) u = p.s_abc[g.abc_of[cell]];
-      const double2 v = p.v_n[cell], a = p.a_n[cell];
-      double2 vh;
-      vh.x = v.x + hdt * a.x;
-      vh.y = v.y + hdt * a.y;
-      up.x = u.x + dt * vh.x;
-      up.y = u.y + dt * vh.y;
-      if (rr >= M && rr < M + kTileRows && cc >= M && cc < M + kTileCols) {
-        p.u_np1[cell] = up;
-        p.vh[cell] = vh;
-        if (ty & kActiveAbc) p.u_n[cell] = u;
-      }
+  const int c = lane;
+#pragma unroll
+  for (int b = 0; b <= M; b++) {
+    constexpr int K = kCellsPerThread;
+    const int A = amax(M, b);
+    // column c + b (P) and c - b (Q), rows r0 - A .. r0 + K - 1 + A
+    double2 P[K + 2 * M], Q[K + 2 * M];
+#pragma unroll
+    for (int t = 0; t < K + 2 * A; t++) {
+      P[t] = su[(r0 - A + t + M) * R::RC + (c + b + M)];
+      Q[t] = (b == 0) ? P[t] : su[(r0 - A + t + M) * R::RC + (c - b + M)];
     }
-    su[q] = up;
-    st[q] = ty;
+#pragma unroll
+    for (int k = 0; k < K; k++)
+#pragma unroll
+      for (int a = -A; a <= A; a++) {
+        if (b == 0 && a <= 0) continue;
+        const int j = sten_index(M, a, b);
+        const double2 up = P[k + A + a], um = Q[k + A - a];
+        s0[k] = fma(SC<M>(5, j), up.x - um.x, s0[k]);
+        s1[k] = fma(SC<M>(6, j), up.y - um.y, s1[k]);
+      }
+  }
+}
+
+template <int M>
+__device__ __forceinline__ double theta_cell_masked(const double2 *__restrict__ su, const uint8_t *__restrict__ sty,
+                                                    int r, int c) {
+  using R = Region<M>;
+  constexpr Sten<M> S = make_sten<M>();
+  const double2 ui = su[(r + M) * R::RC + (c + M)];
+  double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+  for (int j = 0; j < Sten<M>::N; j++) {
+    const int rr = r + M + S.a[j], cc = c + M + S.b[j];
+    if (sty[rr * R::RT + cc] & kExists) {
+      const double2 uj = su[rr * R::RC + cc];
+      s0 = fma(SC<M>(5, j), uj.x - ui.x, s0);
+      s1 = fma(SC<M>(6, j), uj.y - ui.y, s1);
+    }
+  }
+  return s0 + s1;
+}
+
+template <int M>
+__global__ void __launch_bounds__(kTileThreads)
+    k_theta_tma(const __grid_constant__ CUtensorMap map_u, const __grid_constant__ CUtensorMap map_type, Geo g,
+                const DenseTile *__restrict__ tiles, int tile_begin, int n_tiles, StepPtrs p, int pitch,
+                int skip_abc, int *err) {
+  using R = Region<M>;
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem + 2 * R::THETA_STAGE);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (*(volatile int *)err) return;  // an earlier wait timed out: do nothing
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_fence_init();
   }
   __syncthreads();
-  constexpr Sten<M> S = make_sten<M>();
-  const int tx = threadIdx.x & 31, ty0 = threadIdx.x >> 5;
-#pragma unroll 1
-  for (int k = 0; k < kTileRows / 8; k++) {
-    const int r = ty0 + 8 * k;
-    const int q0 = (r + M) * R::RC + (tx + M);
-    const uint8_t tc = st[q0];
-    if (!(tc & kExists)) continue;
-    if (skip_abc && (tc & kActiveAbc)) continue;  // the G_theta warps write it
-    const int cell = t.base + r * pitch + tx;
-    const double2 ui = su[q0];
-    double s0 = 0.0, s1 = 0.0;
-    if (t.full) {
+  auto issue = [&](int stage, int tile) {
+    const DenseTile t = tiles[tile_begin + tile];
+    unsigned char *base = smem + stage * R::THETA_STAGE;
+    mbar_expect_tx(&bar[stage], R::THETA_TX);
+    tma_load_2d(base, &map_u, 2 * t.col, t.row, &bar[stage]);
+    tma_load_2d(base + R::T_TY, &map_type, t.col, t.row, &bar[stage]);
+  };
+  int tile = blockIdx.x;
+  if (tid == 0 && tile < n_tiles) issue(0, tile);
+  for (int it = 0; tile < n_tiles; it++, tile += gridDim.x) {
+    const int stage = it & 1;
+    if (tid == 0 && tile + (int)gridDim.x < n_tiles) issue(stage ^ 1, tile + gridDim.x);
+    const DenseTile t = tiles[tile_begin + tile];
+    const InstParams &P = c_inst[t.inst];
+    double2 *su = reinterpret_cast<double2 *>(smem + stage * R::THETA_STAGE);
+    uint8_t *sty = reinterpret_cast<uint8_t *>(smem + stage * R::THETA_STAGE + R::T_TY);
+    const int r0 = warp * kCellsPerThread;
+    // m_i of the owned cells, fetched while the copy lands
+    double mi[kCellsPerThread];
 #pragma unroll
-      for (int j = 0; j < Sten<M>::N; j++) {
-        const double2 uj = su[q0 + S.a[j] * R::RC + S.b[j]];
-        s0 = fma(SC<M>(5, j), uj.x - ui.x, s0);
-        s1 = fma(SC<M>(6, j), uj.y - ui.y, s1);
+    for (int k = 0; k < kCellsPerThread; k++)
+      mi[k] = g.m[(size_t)(t.row + M + r0 + k) * pitch + t.col + M + lane];
+    if (!mbar_wait_bounded(&bar[stage], (it >> 1) & 1, err)) return;
+    if (t.flags & kTileAbc) {
+      // ABC nodes: u^n from the last G_u, predicted here (src/main.cpp:727)
+      for (int q = tid; q < R::CELLS; q += kTileThreads) {
+        const int rr = q / R::RC, cc = q - rr * R::RC;
+        if (!(sty[rr * R::RT + cc] & kActiveAbc)) continue;
+        const size_t cell = (size_t)(t.row + rr) * pitch + t.col + cc;
+        const double2 u = p.s_abc[g.abc_of[cell]], v = p.v_n[cell], a = p.a_n[cell];
+        double2 vh, up;
+        vh.x = v.x + P.half_dt * a.x;
+        vh.y = v.y + P.half_dt * a.y;
+        up.x = u.x + P.dt * vh.x;
+        up.y = u.y + P.dt * vh.y;
+        su[q] = up;
+        if (rr >= M && rr < M + kTileRows && cc >= M && cc < M + kTileCols) {
+          p.u_np1[cell] = up;
+          p.vh[cell] = vh;
+          p.u_n[cell] = u;
+        }
       }
+      __syncthreads();
+    }
+    double th[kCellsPerThread];
+    if (t.flags & kTileFull) {
+      double2 ui[kCellsPerThread];
+      double s0[kCellsPerThread], s1[kCellsPerThread];
+#pragma unroll
+      for (int k = 0; k < kCellsPerThread; k++) {
+        s0[k] = s1[k] = 0.0;
+        ui[k] = su[(r0 + k + M) * R::RC + lane + M];
+      }
+      theta_tile_full<M>(su, lane, r0, ui, s0, s1);
+#pragma unroll
+      for (int k = 0; k < kCellsPerThread; k++) th[k] = s0[k] + s1[k];
     } else {
-#pragma unroll
-      for (int j = 0; j < Sten<M>::N; j++) {
-        const int q = q0 + S.a[j] * R::RC + S.b[j];
-        if (st[q] & kExists) {
-          const double2 uj = su[q];
-          s0 = fma(SC<M>(5, j), uj.x - ui.x, s0);
-          s1 = fma(SC<M>(6, j), uj.y - ui.y, s1);
-        }
-      }
+#pragma unroll 1
+      for (int k = 0; k < kCellsPerThread; k++)
+        th[k] = (sty[(r0 + k + M) * R::RT + lane + M] & kExists) ? theta_cell_masked<M>(su, sty, r0 + k, lane) : 0.0;
     }
-    const double mi = g.m[cell];
-    p.th_np1[cell] = (mi > 0.0) ? (2.0 / mi) * (s0 + s1) : 0.0;
+#pragma unroll
+    for (int k = 0; k < kCellsPerThread; k++) {
+      const uint8_t ty = sty[(r0 + k + M) * R::RT + lane + M];
+      if (!(ty & kExists)) continue;
+      if (skip_abc && (ty & kActiveAbc)) continue;  // the G_theta kernel writes it
+      const size_t cell = (size_t)(t.row + M + r0 + k) * pitch + t.col + M + lane;
+      p.th_np1[cell] = (mi[k] > 0.0) ? (2.0 / mi[k]) * th[k] : 0.0;
+    }
+    fence_proxy_async_smem();
+    __syncthreads();  // the stage is refilled at the start of the next-but-one iteration
   }
 }
 
-// Force + corrector.  Staged per cell: predicted u, A = 2(l-m)/m theta,
-// B = 8 mu / m and a validity byte (exists and m > 0, src/main.cpp:852).
+// ---------------------------------------------------------------------------
+// Force + corrector + next predictor, persistent over tiles.  After the copy
+// lands, theta is turned into A = 2(l-m)/m theta in place and invalid
+// neighbours (m <= 0, src/main.cpp:852) get A = B = 0 and a cleared bit.
+constexpr uint8_t kForceValid = 0x80;
+
 template <int M>
-__global__ void __launch_bounds__(256)
-    k_force_dense(Geo g, Abc ab, const DenseTile *__restrict__ tiles, StepPtrs p, int tile_begin,
-                  int n_tiles, int abc_on, int bump_step, int *d_step) {
-  // blocks past the tiles exist only in the first group's launch
-  if ((int)blockIdx.x >= n_tiles) {
-    const int a = (blockIdx.x - n_tiles) * kAbcWarpsPerBlock + (threadIdx.x >> 5);
-    abc_uv_warp(ab, a, p);
-    return;
-  }
-  if (bump_step && blockIdx.x == 0 && threadIdx.x == 0) *d_step += 1;
+__device__ __forceinline__ void force_tile_full(const double2 *__restrict__ su, const double *__restrict__ sA,
+                                                const double2 *__restrict__ sco, int lane, int r0, const double2 ui[4],
+                                                const double Bi[4], double F0[4], double F1[4]) {
   using R = Region<M>;
-  extern __shared__ __align__(16) unsigned char smem[];
-  double2 *su = reinterpret_cast<double2 *>(smem);
-  double *sA = reinterpret_cast<double *>(su + R::CELLS);
-  double *sB = sA + R::CELLS;
-  uint8_t *sv = reinterpret_cast<uint8_t *>(sB + R::CELLS);
-  const DenseTile t = tiles[tile_begin + blockIdx.x];
-  const InstParams &P = c_inst[t.inst];
-  const int pitch = P.pitch;
-  for (int q = threadIdx.x; q < R::CELLS; q += 256) {
-    const int rr = q / R::RC, cc = q - rr * R::RC;
-    const int cell = t.base + (rr - M) * pitch + (cc - M);
-    const uint8_t ty = g.type[cell];
-    double2 u = make_double2(0.0, 0.0);
-    double A = 0.0, B = 0.0;
-    uint8_t valid = 0;
-    if (ty & kExists) {
-      const double2 c = g.coef[cell];
-      u = p.u_np1[cell];
-      if (c.y >= 0.0) {
-        A = c.x * p.th_np1[cell];
-        B = c.y;
-        valid = 1;
+  const int c = lane;
+#pragma unroll
+  for (int b = 0; b <= M; b++) {
+    constexpr int K = kCellsPerThread;
+    const int A = amax(M, b);
+    double2 Pu[K + 2 * M], Qu[K + 2 * M];
+    double PA[K + 2 * M], QA[K + 2 * M], PB[K + 2 * M], QB[K + 2 * M];
+#pragma unroll
+    for (int t = 0; t < K + 2 * A; t++) {
+      const int qp = (r0 - A + t + M) * R::RC + (c + b + M);
+      Pu[t] = su[qp];
+      PA[t] = sA[qp];
+      PB[t] = sco[qp].y;
+      if (b == 0) {
+        Qu[t] = Pu[t];
+        QA[t] = PA[t];
+        QB[t] = PB[t];
+      } else {
+        const int qm = (r0 - A + t + M) * R::RC + (c - b + M);
+        Qu[t] = su[qm];
+        QA[t] = sA[qm];
+        QB[t] = sco[qm].y;
       }
     }
-    su[q] = u;
-    sA[q] = A;
-    sB[q] = B;
-    sv[q] = valid;
+#pragma unroll
+    for (int k = 0; k < K; k++)
+#pragma unroll
+      for (int a = -A; a <= A; a++) {
+        if (b == 0 && a <= 0) continue;
+        const int j = sten_index(M, a, b);
+        const double2 up = Pu[k + A + a], um = Qu[k + A - a];
+        // pair (a, b) / (-a, -b): f = g [ (A+ - A-) L + (B_i + B+) e+ - (B_i + B-) e- ]
+        const double e1 = SC<M>(0, j) * (up.x - ui[k].x) + SC<M>(1, j) * (up.y - ui[k].y);
+        const double e2 = SC<M>(0, j) * (ui[k].x - um.x) + SC<M>(1, j) * (ui[k].y - um.y);
+        double T = (PA[k + A + a] - QA[k + A - a]) * SC<M>(2, j);
+        T = fma(Bi[k] + PB[k + A + a], e1, T);
+        T = fma(-(Bi[k] + QB[k + A - a]), e2, T);
+        F0[k] = fma(T, SC<M>(3, j), F0[k]);
+        F1[k] = fma(T, SC<M>(4, j), F1[k]);
+      }
+  }
+}
+
+template <int M>
+__device__ __forceinline__ double2 force_cell_masked(const double2 *__restrict__ su, const double *__restrict__ sA,
+                                                     const double2 *__restrict__ sco, const uint8_t *__restrict__ sty,
+                                                     int r, int c) {
+  using R = Region<M>;
+  constexpr Sten<M> S = make_sten<M>();
+  const int q0 = (r + M) * R::RC + (c + M);
+  const double2 ui = su[q0];
+  const double Ai = sA[q0], Bi = sco[q0].y;
+  double F0 = 0.0, F1 = 0.0;
+#pragma unroll
+  for (int j = 0; j < Sten<M>::N; j++) {
+    const int rr = r + M + S.a[j], cc = c + M + S.b[j];
+    if (sty[rr * R::RT + cc] & kForceValid) {
+      const int q = rr * R::RC + cc;
+      const double2 uj = su[q];
+      const double e = SC<M>(0, j) * (uj.x - ui.x) + SC<M>(1, j) * (uj.y - ui.y);
+      const double T = (Ai + sA[q]) * SC<M>(2, j) + (Bi + sco[q].y) * e;
+      F0 = fma(T, SC<M>(3, j), F0);
+      F1 = fma(T, SC<M>(4, j), F1);
+    }
+  }
+  return make_double2(F0, F1);
+}
+
+template <int M>
+__global__ void __launch_bounds__(kTileThreads)
+    k_force_tma(const __grid_constant__ CUtensorMap map_u, const __grid_constant__ CUtensorMap map_th,
+                const __grid_constant__ CUtensorMap map_coef, const __grid_constant__ CUtensorMap map_type, Geo g,
+                const DenseTile *__restrict__ tiles, int tile_begin, int n_tiles, StepPtrs p, int pitch, int abc_on,
+                int bump_step, int *d_step, int *err) {
+  using R = Region<M>;
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem + 2 * R::FORCE_STAGE);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (*(volatile int *)err) return;  // an earlier wait timed out: do nothing
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_fence_init();
+    if (bump_step && blockIdx.x == 0) *d_step += 1;
   }
   __syncthreads();
-  constexpr Sten<M> S = make_sten<M>();
-  const int tx = threadIdx.x & 31, ty0 = threadIdx.x >> 5;
-#pragma unroll 1
-  for (int k = 0; k < kTileRows / 8; k++) {
-    const int r = ty0 + 8 * k;
-    const int q0 = (r + M) * R::RC + (tx + M);
-    const int cell = t.base + r * pitch + tx;
-    const uint8_t tc = g.type[cell];
-    if (!(tc & kExists)) continue;
-    double2 acc = make_double2(0.0, 0.0);
-    if (sv[q0]) {  // m_i > 0 (:827-831)
-      const double2 ui = su[q0];
-      const double Ai = sA[q0], Bi = sB[q0];
-      double F0 = 0.0, F1 = 0.0;
-      if (t.full) {
+  auto issue = [&](int stage, int tile) {
+    const DenseTile t = tiles[tile_begin + tile];
+    unsigned char *base = smem + stage * R::FORCE_STAGE;
+    mbar_expect_tx(&bar[stage], R::FORCE_TX);
+    tma_load_2d(base, &map_u, 2 * t.col, t.row, &bar[stage]);
+    tma_load_2d(base + R::F_TH, &map_th, t.col, t.row, &bar[stage]);
+    tma_load_2d(base + R::F_CO, &map_coef, 2 * t.col, t.row, &bar[stage]);
+    tma_load_2d(base + R::F_TY, &map_type, t.col, t.row, &bar[stage]);
+  };
+  int tile = blockIdx.x;
+  if (tid == 0 && tile < n_tiles) issue(0, tile);
+  for (int it = 0; tile < n_tiles; it++, tile += gridDim.x) {
+    const int stage = it & 1;
+    if (tid == 0 && tile + (int)gridDim.x < n_tiles) issue(stage ^ 1, tile + gridDim.x);
+    const DenseTile t = tiles[tile_begin + tile];
+    const InstParams &P = c_inst[t.inst];
+    unsigned char *base = smem + stage * R::FORCE_STAGE;
+    double2 *su = reinterpret_cast<double2 *>(base);
+    double *sA = reinterpret_cast<double *>(base + R::F_TH);
+    double2 *sco = reinterpret_cast<double2 *>(base + R::F_CO);
+    uint8_t *sty = reinterpret_cast<uint8_t *>(base + R::F_TY);
+    const int r0 = warp * kCellsPerThread;
+    // corrector inputs of the owned cells, fetched while the copy lands
+    double2 vh[kCellsPerThread];
 #pragma unroll
-        for (int j = 0; j < Sten<M>::N; j++) {
-          const int q = q0 + S.a[j] * R::RC + S.b[j];
-          const double2 uj = su[q];
-          const double e = SC<M>(0, j) * (uj.x - ui.x) + SC<M>(1, j) * (uj.y - ui.y);
-          const double tt = (Ai + sA[q]) * SC<M>(2, j) + (Bi + sB[q]) * e;
-          F0 = fma(tt, SC<M>(3, j), F0);
-          F1 = fma(tt, SC<M>(4, j), F1);
-        }
+    for (int k = 0; k < kCellsPerThread; k++)
+      vh[k] = p.vh[(size_t)(t.row + M + r0 + k) * pitch + t.col + M + lane];
+    if (!mbar_wait_bounded(&bar[stage], (it >> 1) & 1, err)) return;
+    // theta -> A = 2(l - m)/m_j theta_j; validity bit
+    for (int q = tid; q < R::CELLS; q += kTileThreads) {
+      const int rr = q / R::RC, cc = q - rr * R::RC;
+      const double2 co = sco[q];
+      uint8_t ty = sty[rr * R::RT + cc];
+      if ((ty & kExists) && co.y >= 0.0) {
+        sA[q] = co.x * sA[q];
+        ty |= kForceValid;
       } else {
+        sA[q] = 0.0;
+        sco[q] = make_double2(0.0, 0.0);
+      }
+      sty[rr * R::RT + cc] = ty;
+    }
+    __syncthreads();
+    double2 acc[kCellsPerThread];
+    if (t.flags & kTileFull) {
+      double2 ui[kCellsPerThread];
+      double Bi[kCellsPerThread], F0[kCellsPerThread], F1[kCellsPerThread];
 #pragma unroll
-        for (int j = 0; j < Sten<M>::N; j++) {
-          const int q = q0 + S.a[j] * R::RC + S.b[j];
-          if (sv[q]) {
-            const double2 uj = su[q];
-            const double e = SC<M>(0, j) * (uj.x - ui.x) + SC<M>(1, j) * (uj.y - ui.y);
-            const double tt = (Ai + sA[q]) * SC<M>(2, j) + (Bi + sB[q]) * e;
-            F0 = fma(tt, SC<M>(3, j), F0);
-            F1 = fma(tt, SC<M>(4, j), F1);
-          }
+      for (int k = 0; k < kCellsPerThread; k++) {
+        const int q0 = (r0 + k + M) * R::RC + lane + M;
+        ui[k] = su[q0];
+        Bi[k] = sco[q0].y;
+        F0[k] = F1[k] = 0.0;
+      }
+      force_tile_full<M>(su, sA, sco, lane, r0, ui, Bi, F0, F1);
+#pragma unroll
+      for (int k = 0; k < kCellsPerThread; k++) acc[k] = make_double2(F0[k] / P.rho, F1[k] / P.rho);
+    } else {
+#pragma unroll 1
+      for (int k = 0; k < kCellsPerThread; k++) {
+        acc[k] = make_double2(0.0, 0.0);
+        if (sty[(r0 + k + M) * R::RT + lane + M] & kForceValid) {
+          const double2 F = force_cell_masked<M>(su, sA, sco, sty, r0 + k, lane);
+          acc[k] = make_double2(F.x / P.rho, F.y / P.rho);
         }
       }
-      acc.x = F0 / P.rho;
-      acc.y = F1 / P.rho;
     }
-    p.a_np1[cell] = acc;
-    if (!(abc_on && (tc & kActiveAbc))) {
-      const double2 vh = p.vh[cell];
-      p.v_np1[cell] = make_double2(vh.x + P.half_dt * acc.x, vh.y + P.half_dt * acc.y);
+#pragma unroll
+    for (int k = 0; k < kCellsPerThread; k++) {
+      const uint8_t ty = sty[(r0 + k + M) * R::RT + lane + M];
+      if (!(ty & kExists)) continue;
+      const size_t cell = (size_t)(t.row + M + r0 + k) * pitch + t.col + M + lane;
+      p.a_np1[cell] = acc[k];
+      if (abc_on && (ty & kActiveAbc)) continue;  // G_v writes v; the next theta kernel predicts u
+      // corrector (:924) then the next predictor (:727) from the same values
+      double2 v, vh2, un;
+      v.x = vh[k].x + P.half_dt * acc[k].x;
+      v.y = vh[k].y + P.half_dt * acc[k].y;
+      vh2.x = v.x + P.half_dt * acc[k].x;
+      vh2.y = v.y + P.half_dt * acc[k].y;
+      const double2 u = su[(r0 + k + M) * R::RC + lane + M];
+      un.x = u.x + P.dt * vh2.x;
+      un.y = u.y + P.dt * vh2.y;
+      p.v_np1[cell] = v;
+      p.vh[cell] = vh2;
+      p.u_np2[cell] = un;
     }
+    fence_proxy_async_smem();
+    __syncthreads();
   }
+}
+
+// ---------------------------------------------------------------------------
+// Absorbing-boundary kernels (run concurrently with the tile kernels).
+__global__ void __launch_bounds__(256) k_abc_theta(Abc ab, const double *th_n, const double *th_nm1, double *theta) {
+  const int a = blockIdx.x * kAbcWarpsPerBlock + (threadIdx.x >> 5);
+  abc_theta_warp(ab, a, th_n, th_nm1, theta);
+}
+
+__global__ void __launch_bounds__(256) k_abc_uv(Abc ab, StepPtrs p) {
+  const int a = blockIdx.x * kAbcWarpsPerBlock + (threadIdx.x >> 5);
+  abc_uv_warp(ab, a, p);
 }
 
 // ---------------------------------------------------------------------------
@@ -312,13 +569,13 @@ __global__ void __launch_bounds__(256)
 // diagnostics cadence): theta history init (src/main.cpp:664-682) and the
 // energy/momentum partial sums (:986-1062).
 template <int M>
-__device__ __forceinline__ double theta_cell(const Geo &g, const double2 *u, int cell, int pitch) {
+__device__ __forceinline__ double theta_cell(const Geo &g, const double2 *u, size_t cell, int pitch) {
   constexpr Sten<M> S = make_sten<M>();
   const double2 ui = u[cell];
   double s0 = 0.0, s1 = 0.0;
 #pragma unroll
   for (int j = 0; j < Sten<M>::N; j++) {
-    const int nb = cell + S.a[j] * pitch + S.b[j];
+    const size_t nb = cell + (ptrdiff_t)S.a[j] * pitch + S.b[j];
     if (g.type[nb] & kExists) {
       const double2 uj = u[nb];
       s0 = fma(SC<M>(5, j), uj.x - ui.x, s0);
@@ -329,41 +586,39 @@ __device__ __forceinline__ double theta_cell(const Geo &g, const double2 *u, int
   return (mi > 0.0) ? (2.0 / mi) * (s0 + s1) : 0.0;
 }
 
+template <int M>
+__device__ __forceinline__ void theta_cell_into(const Geo &g, const double2 *u, size_t cell, int pitch, double *out) {
+  *out = theta_cell<M>(g, u, cell, pitch);
+}
+
 __global__ void __launch_bounds__(256) k_theta_dense_init(Geo g, const double2 *u, double *theta) {
-  const int cell = blockIdx.x * 256 + threadIdx.x;
-  if (cell >= g.n_total || !(g.type[cell] & kExists)) return;
+  const size_t cell = (size_t)blockIdx.x * 256 + threadIdx.x;
+  if (cell >= (size_t)g.n_total || !(g.type[cell] & kExists)) return;
   const InstParams &P = c_inst[g.blk_inst[blockIdx.x]];
   double th = 0.0;
-  switch (P.stencil) {
-    case 2: th = theta_cell<2>(g, u, cell, P.pitch); break;
-    case 3: th = theta_cell<3>(g, u, cell, P.pitch); break;
-    case 4: th = theta_cell<4>(g, u, cell, P.pitch); break;
-    case 5: th = theta_cell<5>(g, u, cell, P.pitch); break;
-    case 6: th = theta_cell<6>(g, u, cell, P.pitch); break;
-    case 8: th = theta_cell<8>(g, u, cell, P.pitch); break;
-  }
+  LPS_DISPATCH_M(P.stencil, theta_cell_into, g, u, cell, P.pitch, &th);
   theta[cell] = th;
 }
 
-// Deviatoric strain energy density sum of one cell, src/main.cpp:1025-1038.
+// Deviatoric strain-energy sum of one cell, src/main.cpp:1025-1038.
 template <int M>
-__device__ __forceinline__ double wdev_cell(const Geo &g, const double2 *u, int cell, int pitch, double th,
-                                            double coef) {
+__device__ __forceinline__ void wdev_cell(const Geo &g, const double2 *u, size_t cell, int pitch, double th,
+                                          double coef, double *W) {
   constexpr Sten<M> S = make_sten<M>();
   const double2 ui = u[cell];
-  double W = 0.0;
+  double w = 0.0;
 #pragma unroll
   for (int j = 0; j < Sten<M>::N; j++) {
-    const int nb = cell + S.a[j] * pitch + S.b[j];
+    const size_t nb = cell + (ptrdiff_t)S.a[j] * pitch + S.b[j];
     if (g.type[nb] & kExists) {
       const double2 uj = u[nb];
       const double e = SC<M>(0, j) * (uj.x - ui.x) + SC<M>(1, j) * (uj.y - ui.y);
       const double ed = e - th * SC<M>(2, j) / 2.0;
       const double bdv = SC<M>(3, j) * SC<M>(0, j) + SC<M>(4, j) * SC<M>(1, j);
-      W += coef * ed * ed * bdv;
+      w += coef * ed * ed * bdv;
     }
   }
-  return W;
+  *W = w;
 }
 
 __global__ void __launch_bounds__(kNodeBlock)
@@ -384,28 +639,20 @@ __global__ void __launch_bounds__(kNodeBlock)
     acc.block_reduce_store(partials + blockIdx.x);
     return;
   }
-  const int cell = blockIdx.x * kNodeBlock + threadIdx.x;
-  if (cell < g.n_total && (g.type[cell] & kExists)) {
+  const size_t cell = (size_t)blockIdx.x * kNodeBlock + threadIdx.x;
+  if (cell < (size_t)g.n_total && (g.type[cell] & kExists)) {
     const InstParams &P = c_inst[g.blk_inst[blockIdx.x]];
     const double2 xy = g.xy[cell], un = u[cell], vn = v[cell], an = a[cell];
     const double th = theta[cell];
     const double r = sqrt(xy.x * xy.x + xy.y * xy.y);
-    acc.add_maxima(un, vn, an, th, cell);
+    acc.add_maxima(un, vn, an, th, (int)cell);
     if (!(P.out_r > 0.0 && r > P.out_r)) {
       acc.Px = P.rho * vn.x * P.dx * P.dy;
       acc.Py = P.rho * vn.y * P.dx * P.dy;
       const double ek = 0.5 * P.rho * (vn.x * vn.x + vn.y * vn.y) * P.dx * P.dy;
-      const double m_i = g.m[cell];
-      const double coef = P.c_mu4 / m_i;
+      const double coef = P.c_mu4 / g.m[cell];
       double W = 0.0;
-      switch (P.stencil) {
-        case 2: W = wdev_cell<2>(g, u, cell, P.pitch, th, coef); break;
-        case 3: W = wdev_cell<3>(g, u, cell, P.pitch, th, coef); break;
-        case 4: W = wdev_cell<4>(g, u, cell, P.pitch, th, coef); break;
-        case 5: W = wdev_cell<5>(g, u, cell, P.pitch, th, coef); break;
-        case 6: W = wdev_cell<6>(g, u, cell, P.pitch, th, coef); break;
-        case 8: W = wdev_cell<8>(g, u, cell, P.pitch, th, coef); break;
-      }
+      LPS_DISPATCH_M(P.stencil, wdev_cell, g, u, cell, P.pitch, th, coef, &W);
       const double W_i = 0.5 * P.kappa * th * th + W;
       const double ep = W_i * P.dx * P.dy;
       acc.Ek = ek;
@@ -416,71 +663,184 @@ __global__ void __launch_bounds__(kNodeBlock)
   acc.block_reduce_store(partials + blockIdx.x);
 }
 
-// ---------------------------------------------------------------------------
-template <int M>
-static cudaError_t set_smem_attrs() {
-  cudaError_t e = cudaFuncSetAttribute(k_theta_dense<M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)theta_smem<M>());
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_force_dense<M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)force_smem<M>());
+// u^1 = u^0 + dt (v^0 + dt/2 a^0) with a^0 = 0, and vh = v^0, src/main.cpp:727.
+__global__ void __launch_bounds__(256) k_dense_reset_predict(Geo g, const double2 *u0, const double2 *v0,
+                                                              double2 *u1, double2 *vh) {
+  const size_t cell = (size_t)blockIdx.x * 256 + threadIdx.x;
+  if (cell >= (size_t)g.n_total) return;
+  if (!(g.type[cell] & kExists)) {
+    u1[cell] = make_double2(0.0, 0.0);
+    vh[cell] = make_double2(0.0, 0.0);
+    return;
+  }
+  const InstParams &P = c_inst[g.blk_inst[blockIdx.x]];
+  const double2 u = u0[cell], v = v0[cell];
+  double2 h, up;
+  h.x = v.x + P.half_dt * 0.0;
+  h.y = v.y + P.half_dt * 0.0;
+  up.x = u.x + P.dt * h.x;
+  up.y = u.y + P.dt * h.y;
+  u1[cell] = up;
+  vh[cell] = h;
 }
 
-cudaError_t dense_prepare_kernels() {
+// ---------------------------------------------------------------------------
+// host side
+template <int M>
+static cudaError_t prepare_m(DenseGroup &gr, int n_sm) {
   cudaError_t e;
-  if ((e = set_smem_attrs<2>()) || (e = set_smem_attrs<3>()) || (e = set_smem_attrs<4>()) ||
-      (e = set_smem_attrs<5>()) || (e = set_smem_attrs<6>()) || (e = set_smem_attrs<8>()))
+  if ((e = cudaFuncSetAttribute(k_theta_tma<M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                Region<M>::THETA_SMEM)))
     return e;
+  if ((e = cudaFuncSetAttribute(k_force_tma<M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                Region<M>::FORCE_SMEM)))
+    return e;
+  int bt = 0, bf = 0;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, k_theta_tma<M>, kTileThreads, Region<M>::THETA_SMEM)))
+    return e;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf, k_force_tma<M>, kTileThreads, Region<M>::FORCE_SMEM)))
+    return e;
+  bt = std::max(bt, 1);
+  bf = std::max(bf, 1);
+  gr.grid_theta = std::min(gr.n_tiles, bt * n_sm);
+  gr.grid_force = std::min(gr.n_tiles, bf * n_sm);
   return cudaSuccess;
 }
 
 template <int M>
-static void launch_group(const DenseGroup &gr, bool first, const LaunchGeo &lg, const DenseGeo &dg,
-                         const StepPtrs &p, int *d_step, cudaStream_t st, const Mark *mark) {
-  const bool gth = lg.abcs_step != -1 && lg.abc.n_abc > 0 && lg.theta_method == 1;
-  const int extra = (first && gth) ? lg.n_abc_blocks : 0;
-  k_theta_dense<M><<<gr.n_tiles + extra, 256, theta_smem<M>(), st>>>(lg.geo, lg.abc, dg.tiles, p,
-                                                                     gr.tile_begin, gr.n_tiles, gth ? 1 : 0);
-  if (mark) (*mark)("theta_dense");
+static void prepare_dispatch(DenseGroup &gr, int n_sm, cudaError_t *e) {
+  *e = prepare_m<M>(gr, n_sm);
+}
+
+cudaError_t dense_prepare(DenseGeo &dg) {
+  int dev = 0, n_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+  for (auto &gr : dg.groups) {
+    cudaError_t e = cudaErrorInvalidValue;
+    LPS_DISPATCH_M(gr.m, prepare_dispatch, gr, n_sm, &e);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+namespace {
+PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+bool encode(CUtensorMap *map, CUtensorMapDataType dt, size_t elem, const void *base, uint64_t inner,
+            uint64_t rows, uint32_t box_inner, uint32_t box_rows) {
+  auto fn = get_encode();
+  if (!fn) return false;
+  const cuuint64_t dims[2] = {inner, rows};
+  const cuuint64_t strides[1] = {inner * elem};
+  const cuuint32_t box[2] = {box_inner, box_rows};
+  const cuuint32_t estr[2] = {1, 1};
+  return fn(map, dt, 2, const_cast<void *>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 template <int M>
-static void launch_force_group(const DenseGroup &gr, bool first, const LaunchGeo &lg, const DenseGeo &dg,
-                               const StepPtrs &p, int *d_step, cudaStream_t st, const Mark *mark) {
-  const bool abc_on = lg.abcs_step != -1 && lg.abc.n_abc > 0;
-  const int extra = (first && abc_on) ? lg.n_abc_blocks : 0;
-  k_force_dense<M><<<gr.n_tiles + extra, 256, force_smem<M>(), st>>>(
-      lg.geo, lg.abc, dg.tiles, p, gr.tile_begin, gr.n_tiles, abc_on ? 1 : 0, first ? 1 : 0, d_step);
-  if (mark) (*mark)("force_dense");
+void encode_m(DenseGroup &g, int pitch, int rows, double2 *const *U, double *const *TH, const double2 *coef,
+              const uint8_t *type, bool *ok) {
+  using R = Region<M>;
+  bool good = true;
+  for (int r = 0; r < kUring; r++)
+    good &= encode(&g.maps.u[r], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, U[r], 2ull * pitch, rows, 2 * R::RC, R::RR);
+  for (int r = 0; r < 3; r++)
+    good &= encode(&g.maps.th[r], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, TH[r], pitch, rows, R::RC, R::RR);
+  good &= encode(&g.maps.coef, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, coef, 2ull * pitch, rows, 2 * R::RC, R::RR);
+  good &= encode(&g.maps.type, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, type, pitch, rows, R::RT, R::RR);
+  *ok = good;
+}
+}  // namespace
+
+int dense_encode_maps(DenseGroup &g, int pitch, int total_rows, double2 *const *U, double *const *TH,
+                      const double2 *coef, const uint8_t *type, std::string &err) {
+  bool ok = false;
+  LPS_DISPATCH_M(g.m, encode_m, g, pitch, total_rows, U, TH, coef, type, &ok);
+  if (!ok) {
+    err = "cuTensorMapEncodeTiled failed for the dense layout";
+    return LPS_ERR_CUDA;
+  }
+  return LPS_OK;
 }
 
-#define LPS_DISPATCH_M(m, FN, ...)          \
-  switch (m) {                              \
-    case 2: FN<2>(__VA_ARGS__); break;      \
-    case 3: FN<3>(__VA_ARGS__); break;      \
-    case 4: FN<4>(__VA_ARGS__); break;      \
-    case 5: FN<5>(__VA_ARGS__); break;      \
-    case 6: FN<6>(__VA_ARGS__); break;      \
-    case 8: FN<8>(__VA_ARGS__); break;      \
-  }
+template <int M>
+static void launch_theta_group(const DenseGroup &gr, const LaunchGeo &lg, const DenseGeo &dg, const StepPtrs &p,
+                               int ring_u, bool skip_abc, cudaStream_t st) {
+  k_theta_tma<M><<<gr.grid_theta, kTileThreads, Region<M>::THETA_SMEM, st>>>(
+      gr.maps.u[ring_u], gr.maps.type, lg.geo, dg.tiles, gr.tile_begin, gr.n_tiles, p, dg.pitch, skip_abc ? 1 : 0,
+      dg.d_err);
+}
 
+template <int M>
+static void launch_force_group(const DenseGroup &gr, const LaunchGeo &lg, const DenseGeo &dg, const StepPtrs &p,
+                               int ring_u, int ring_th, bool abc_on, bool first, int *d_step, cudaStream_t st) {
+  k_force_tma<M><<<gr.grid_force, kTileThreads, Region<M>::FORCE_SMEM, st>>>(
+      gr.maps.u[ring_u], gr.maps.th[ring_th], gr.maps.coef, gr.maps.type, lg.geo, dg.tiles, gr.tile_begin,
+      gr.n_tiles, p, dg.pitch, abc_on ? 1 : 0, first ? 1 : 0, d_step, dg.d_err);
+}
+
+// ring_u: index of u^{n+1} (the predicted level) in the 4-deep ring;
+// p.th_np1 is theta^{n+1}, whose ring index is ring_u' = (n+1) % 3.
 int enqueue_dense_step(const DenseGeo &dg, const LaunchGeo &lg, const StepPtrs &p, int *d_step,
-                       cudaStream_t st, const Mark *mark) {
+                       cudaStream_t st, const Mark *mark, int ring_u) {
   int k = 0;
-  for (size_t i = 0; i < dg.groups.size(); i++) {
-    LPS_DISPATCH_M(dg.groups[i].m, launch_group, dg.groups[i], i == 0, lg, dg, p, d_step, st, mark);
+  const bool abc = lg.abcs_step != -1 && lg.abc.n_abc > 0;
+  const bool gth = abc && lg.theta_method == 1;
+  const int rth = p.th_ring;
+  // pass 1: theta tiles || G_theta
+  if (gth) {
+    cudaEventRecord(dg.ev_fork[0], st);
+    cudaStreamWaitEvent(dg.side, dg.ev_fork[0], 0);
+    k_abc_theta<<<lg.n_abc_blocks, 256, 0, dg.side>>>(lg.abc, p.th_n, p.th_nm1, p.th_np1);
+    cudaEventRecord(dg.ev_join[0], dg.side);
     k++;
   }
-  if (lg.abcs_step != -1 && lg.theta_method == 0 && lg.abc.n_abc > 0) {
+  for (const auto &gr : dg.groups) {
+    LPS_DISPATCH_M(gr.m, launch_theta_group, gr, lg, dg, p, ring_u, gth, st);
+    k++;
+  }
+  if (gth) cudaStreamWaitEvent(st, dg.ev_join[0], 0);
+  if (mark) (*mark)("theta_dense");
+  if (abc && lg.theta_method == 0) {
     launch_theta_idw(lg, p.th_np1, st);
     if (mark) (*mark)("theta_idw");
     k++;
   }
-  for (size_t i = 0; i < dg.groups.size(); i++) {
-    LPS_DISPATCH_M(dg.groups[i].m, launch_force_group, dg.groups[i], i == 0, lg, dg, p, d_step, st, mark);
+  // pass 2: force tiles || G_u, G_v
+  if (abc) {
+    cudaEventRecord(dg.ev_fork[1], st);
+    cudaStreamWaitEvent(dg.side, dg.ev_fork[1], 0);
+    k_abc_uv<<<lg.n_abc_blocks, 256, 0, dg.side>>>(lg.abc, p);
+    cudaEventRecord(dg.ev_join[1], dg.side);
     k++;
   }
+  bool first = true;
+  for (const auto &gr : dg.groups) {
+    LPS_DISPATCH_M(gr.m, launch_force_group, gr, lg, dg, p, ring_u, rth, abc, first, d_step, st);
+    first = false;
+    k++;
+  }
+  if (abc) cudaStreamWaitEvent(st, dg.ev_join[1], 0);
+  if (mark) (*mark)("force_dense");
   return k;
+}
+
+void launch_dense_reset_predict(const LaunchGeo &lg, const double2 *u0, const double2 *v0, double2 *u1,
+                                double2 *vh, cudaStream_t st) {
+  k_dense_reset_predict<<<lg.n_node_blocks, 256, 0, st>>>(lg.geo, u0, v0, u1, vh);
 }
 
 void launch_theta_dense_init(const DenseGeo &, const LaunchGeo &lg, const double2 *u, double *theta,
