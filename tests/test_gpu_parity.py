@@ -100,7 +100,9 @@ def test_batch_equals_single(path):
         d1, st1, _, _ = run_gpu(s, path, n_steps=60, diag_every=6)
         for key in ("u", "v", "a", "theta"):
             np.testing.assert_array_equal(batch[k][1][key], st1[key])
-        np.testing.assert_array_equal(batch[k][0]["E"], d1["E"])
+        # the dense batch shares one row pitch, so the reduction tree groups
+        # cells differently than a single instance: equal up to rounding
+        np.testing.assert_allclose(batch[k][0]["E"], d1["E"], rtol=1e-13, atol=0)
 
 
 @pytest.mark.parametrize("path", PATHS)
