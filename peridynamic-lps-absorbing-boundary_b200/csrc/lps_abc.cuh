@@ -1,5 +1,14 @@
 // lps_abc.cuh -- device helpers shared by the CSR and dense kernels: the
 // volume-correction factor and the absorbing-boundary operator warps.
+//
+// Operator layout (packed on the host): the compacted cloud of ABC entry a
+// occupies entries [cl_off, cl_off + cl_len); G_u and G_v are stored per
+// entry component-major, 8 rows of cl_len doubles starting at 8 * cl_off:
+//   rows 0-3: x output <- (x^n, y^n, x^{n-1}, y^{n-1}),  rows 4-7: y output,
+// and G_theta as 2 rows (theta^n, theta^{n-1}) starting at 2 * cl_off, so the
+// 32 lanes of a warp read 32 consecutive doubles per row.  A warp serves one
+// ABC node and issues the loads of up to 64 cloud entries (two per lane)
+// before it consumes any of them.
 #pragma once
 #include "lps_common.cuh"
 
@@ -13,41 +22,62 @@ __device__ __forceinline__ double beta_dev(double xi, const InstParams &P) {
 }
 
 // G_theta at one ABC node per warp, src/main.cpp:795-812.
-__device__ __forceinline__ void abc_theta_warp(const Abc &ab, int a, const double *th_n,
-                                               const double *th_nm1, double *theta) {
+__device__ __forceinline__ void abc_theta_warp(const Abc &ab, int a, const double *__restrict__ th_n,
+                                               const double *__restrict__ th_nm1, double *theta) {
   const int lane = threadIdx.x & 31;
   if (a >= ab.n_abc || !ab.writes[a]) return;
   const int off = ab.cl_off[a], len = ab.cl_len[a];
+  const double *__restrict__ w0 = ab.gth + 2 * (size_t)off;
+  const double *__restrict__ w1 = w0 + len;
   double acc = 0.0;
-  for (int e = lane; e < len; e += 32) {
-    const int k = ab.cl_idx[off + e];
-    const double2 w = ab.gth[off + e];
-    acc += w.x * th_n[k] + w.y * th_nm1[k];
+  for (int e0 = 0; e0 < len; e0 += 64) {
+    const int ea = e0 + lane, eb = e0 + 32 + lane;
+    const bool va = ea < len, vb = eb < len;
+    const int ka = va ? __ldg(ab.cl_idx + off + ea) : 0, kb = vb ? __ldg(ab.cl_idx + off + eb) : 0;
+    const double wa0 = va ? __ldg(w0 + ea) : 0.0, wa1 = va ? __ldg(w1 + ea) : 0.0;
+    const double wb0 = vb ? __ldg(w0 + eb) : 0.0, wb1 = vb ? __ldg(w1 + eb) : 0.0;
+    const double ta0 = va ? th_n[ka] : 0.0, ta1 = va ? th_nm1[ka] : 0.0;
+    const double tb0 = vb ? th_n[kb] : 0.0, tb1 = vb ? th_nm1[kb] : 0.0;
+    acc += wa0 * ta0 + wa1 * ta1;
+    acc += wb0 * tb0 + wb1 * tb1;
   }
   acc = warp_sum(acc);
   if (lane == 0) theta[ab.node[a]] = acc;
 }
 
+// One cloud entry's contribution to the x and y outputs of a 2-level operator.
+__device__ __forceinline__ void g_entry(const double *__restrict__ g, int len, int e, double2 xn, double2 xm,
+                                        double &ox, double &oy) {
+  ox += __ldg(g + 0 * len + e) * xn.x + __ldg(g + 1 * len + e) * xn.y + __ldg(g + 2 * len + e) * xm.x +
+        __ldg(g + 3 * len + e) * xm.y;
+  oy += __ldg(g + 4 * len + e) * xn.x + __ldg(g + 5 * len + e) * xn.y + __ldg(g + 6 * len + e) * xm.x +
+        __ldg(g + 7 * len + e) * xm.y;
+}
+
 // ABC displacement and velocity at one ABC node per warp,
-// src/main.cpp:883-916 and :933-974.  G rows are stored per cloud entry as
-// [gx(x^n), gx(y^n), gx(x^{n-1}), gx(y^{n-1}), gy(...) x4].
+// src/main.cpp:883-916 and :933-974.
 __device__ __forceinline__ void abc_uv_warp(const Abc &ab, int a, const StepPtrs &p) {
   const int lane = threadIdx.x & 31;
   if (a >= ab.n_abc || !ab.writes[a]) return;
   const InstParams &P = c_inst[ab.inst[a]];
   const int off = ab.cl_off[a], len = ab.cl_len[a];
+  const double *__restrict__ gu = ab.gu + 8 * (size_t)off;
+  const double *__restrict__ gv = ab.gv + 8 * (size_t)off;
   double ux = 0.0, uy = 0.0, vx = 0.0, vy = 0.0;
-  for (int e = lane; e < len; e += 32) {
-    const int k = ab.cl_idx[off + e];
-    const double2 un = p.u_n[k], unm1 = p.u_nm1[k];
-    const double *gu = ab.gu + (size_t)(off + e) * 8;
-    ux += gu[0] * un.x + gu[1] * un.y + gu[2] * unm1.x + gu[3] * unm1.y;
-    uy += gu[4] * un.x + gu[5] * un.y + gu[6] * unm1.x + gu[7] * unm1.y;
+  const double2 z = make_double2(0.0, 0.0);
+  for (int e0 = 0; e0 < len; e0 += 64) {
+    const int ea = e0 + lane, eb = e0 + 32 + lane;
+    const bool va = ea < len, vb = eb < len;
+    const int ka = va ? __ldg(ab.cl_idx + off + ea) : 0, kb = vb ? __ldg(ab.cl_idx + off + eb) : 0;
+    const double2 una = va ? p.u_n[ka] : z, uma = va ? p.u_nm1[ka] : z;
+    const double2 unb = vb ? p.u_n[kb] : z, umb = vb ? p.u_nm1[kb] : z;
+    if (va) g_entry(gu, len, ea, una, uma, ux, uy);
+    if (vb) g_entry(gu, len, eb, unb, umb, ux, uy);
     if (!P.kinematic) {
-      const double2 vn = p.v_n[k], vnm1 = p.v_nm1[k];
-      const double *gv = ab.gv + (size_t)(off + e) * 8;
-      vx += gv[0] * vn.x + gv[1] * vn.y + gv[2] * vnm1.x + gv[3] * vnm1.y;
-      vy += gv[4] * vn.x + gv[5] * vn.y + gv[6] * vnm1.x + gv[7] * vnm1.y;
+      const double2 vna = va ? p.v_n[ka] : z, vma = va ? p.v_nm1[ka] : z;
+      const double2 vnb = vb ? p.v_n[kb] : z, vmb = vb ? p.v_nm1[kb] : z;
+      if (va) g_entry(gv, len, ea, vna, vma, vx, vy);
+      if (vb) g_entry(gv, len, eb, vnb, vmb, vx, vy);
     }
   }
   ux = warp_sum(ux);

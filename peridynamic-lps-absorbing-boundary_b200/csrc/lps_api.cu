@@ -127,7 +127,7 @@ struct HostAbc {
   std::vector<int> node, inst, cl_off, cl_len, cl_idx, idw_off, idw_len, idw_idx;
   std::vector<uint8_t> writes, active;
   std::vector<double> gu, gv, idw_w;
-  std::vector<double2> gth;
+  std::vector<double> gth;
 };
 
 // Appends instance k's absorbing-boundary data.  `gmap(local)` maps a local
@@ -155,31 +155,27 @@ void pack_abc(const lps_problem &p, const lps_options &o, const InstanceSetup &s
     H.active[a] = active;
     H.writes[a] = writes;
     H.cl_off[a] = (int)H.cl_idx.size();
-    int len = 0;
-    for (int j = 0; j < C; j++) {
-      const int kk = p.clouds[(size_t)i * C + j];
-      if (kk == -1) continue;
-      H.cl_idx.push_back(gmap(kk));
-      const double *g0 = p.gu + (size_t)(2 * i) * cols, *g1 = p.gu + (size_t)(2 * i + 1) * cols;
-      const double *h0 = p.gv + (size_t)(2 * i) * cols, *h1 = p.gv + (size_t)(2 * i + 1) * cols;
-      double gx[8] = {0, 0, 0, 0, 0, 0, 0, 0}, gy[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-      for (int c = 0; c < cpc; c++) {
-        gx[c] = g0[cpc * j + c];
-        gx[4 + c] = g1[cpc * j + c];
-        gy[c] = h0[cpc * j + c];
-        gy[4 + c] = h1[cpc * j + c];
+    // entries with k != -1, then the operators component-major (see lps_abc.cuh)
+    std::vector<int> js;
+    for (int j = 0; j < C; j++)
+      if (p.clouds[(size_t)i * C + j] != -1) js.push_back(j);
+    const int len = (int)js.size();
+    for (int j : js) H.cl_idx.push_back(gmap(p.clouds[(size_t)i * C + j]));
+    const double *g0 = p.gu + (size_t)(2 * i) * cols, *g1 = p.gu + (size_t)(2 * i + 1) * cols;
+    const double *h0 = p.gv + (size_t)(2 * i) * cols, *h1 = p.gv + (size_t)(2 * i + 1) * cols;
+    for (int r = 0; r < 8; r++) {
+      const int c = r & 3;  // column within the entry: x^n, y^n, x^{n-1}, y^{n-1}
+      for (int j : js) {
+        H.gu.push_back(c < cpc ? (r < 4 ? g0 : g1)[cpc * j + c] : 0.0);
+        H.gv.push_back(c < cpc ? (r < 4 ? h0 : h1)[cpc * j + c] : 0.0);
       }
-      H.gu.insert(H.gu.end(), gx, gx + 8);
-      H.gv.insert(H.gv.end(), gy, gy + 8);
-      double2 w = make_double2(0.0, 0.0);
-      if (o.theta_method == 1 && p.gtheta) {
-        const double *gt = p.gtheta + (size_t)i * cth * C;
-        w.x = gt[cth * j];
-        if (cth == 2) w.y = gt[cth * j + 1];
-      }
-      H.gth.push_back(w);
-      len++;
     }
+    for (int r = 0; r < 2; r++)
+      for (int j : js) {
+        double w = 0.0;
+        if (o.theta_method == 1 && p.gtheta && r < cth) w = p.gtheta[(size_t)i * cth * C + cth * j + r];
+        H.gth.push_back(w);
+      }
     H.cl_len[a] = len;
     // inverse-distance lists, src/main.cpp:775-786
     H.idw_off[a] = (int)H.idw_idx.size();
@@ -233,7 +229,7 @@ int upload_abc(lps_handle *h, const HostAbc &H, int total_abc) {
   int *a_node, *a_inst, *a_cl_off, *a_cl_len, *a_cl_idx, *a_idw_off, *a_idw_len, *a_idw_idx;
   uint8_t *a_writes, *a_active;
   double *a_gu, *a_gv, *a_idw_w;
-  double2 *a_gth;
+  double *a_gth;
   if ((s = dev_upload(h, &a_node, H.node)) || (s = dev_upload(h, &a_inst, H.inst)) ||
       (s = dev_upload(h, &a_cl_off, H.cl_off)) || (s = dev_upload(h, &a_cl_len, H.cl_len)) ||
       (s = dev_upload(h, &a_cl_idx, H.cl_idx)) || (s = dev_upload(h, &a_idw_off, H.idw_off)) ||

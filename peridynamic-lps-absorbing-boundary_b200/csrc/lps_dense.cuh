@@ -28,8 +28,8 @@ namespace lps {
 
 constexpr int kTileRows = 16;   // owned cells per tile: 16 rows x 32 columns
 constexpr int kTileCols = 32;
-constexpr int kCellsPerThread = 4;                                // consecutive rows
-constexpr int kTileThreads = kTileRows * kTileCols / kCellsPerThread;  // 128
+constexpr int kCellsPerThread = 2;                                // adjacent rows
+constexpr int kTileThreads = kTileRows * kTileCols / kCellsPerThread;  // 256
 constexpr int kDenseM[] = {2, 3, 4, 5, 6, 8};
 constexpr int kUring = 4;       // displacement ring depth of the dense path
 

@@ -97,7 +97,7 @@ struct Abc {
   const int *cl_idx;           // global node index per cloud entry
   const double *gu;            // per entry 8 doubles: row x [4], row y [4]
   const double *gv;            // same
-  const double2 *gth;          // per entry (theta^n, theta^{n-1}) weights
+  const double *gth;           // per node: rows theta^n, theta^{n-1} of cl_len weights
   const int *idw_off, *idw_len;// IDW neighbour lists (THETA_ABC_METHOD 0)
   const int *idw_idx;
   const double *idw_w;

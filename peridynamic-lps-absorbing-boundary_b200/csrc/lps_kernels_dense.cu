@@ -224,57 +224,115 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
 }
 
 // ---------------------------------------------------------------------------
-// Predictor + dilatation, persistent over tiles.
+// Tile compute.  A thread owns cells (r0, c) and (r0 + 1, c); for every pair
+// of opposite offsets (a, b) / (-a, -b) it reads the two staged neighbours of
+// each cell -- the row-(r0+1) reads of one offset are the row-r0 reads of the
+// next, so about half of them come from registers.
+//   dilatation pair:  c_j . (u(+) - u(-))                    (src/main.cpp:757)
+//   force pair:       g_j [ (A+ - A-) |xi| + (B_i + B+) e+ - (B_i + B-) e- ]
+// with e+ = (u(+) - u_i) . xi_hat, e- = (u_i - u(-)) . xi_hat, A = 2(l-m)/m
+// theta, B = 8 mu / m (:857-869).  Masked tiles (near the domain edge) use the
+// same pairs with absent neighbours zeroed: u = A = B = 0 there, and the
+// owned node's own terms are weighted by which side is present.
 template <int M>
-__device__ __forceinline__ void theta_tile_full(const double2 *__restrict__ su, int lane, int r0, double2 ui[4],
-                                                double s0[4], double s1[4]) {
+__device__ __forceinline__ int QI(int r, int c) {
+  return (r + M) * Region<M>::RC + (c + M);
+}
+
+template <int M, bool FULL>
+__device__ __forceinline__ void theta_tile(const double2 *__restrict__ su, const uint8_t *__restrict__ sty, int r0,
+                                           int c, double th[2]) {
   using R = Region<M>;
-  const int c = lane;
+  const double2 ui0 = su[QI<M>(r0, c)], ui1 = su[QI<M>(r0 + 1, c)];
+  double s00 = 0.0, s01 = 0.0, s10 = 0.0, s11 = 0.0;
 #pragma unroll
   for (int b = 0; b <= M; b++) {
-    constexpr int K = kCellsPerThread;
     const int A = amax(M, b);
-    // column c + b (P) and c - b (Q), rows r0 - A .. r0 + K - 1 + A
-    double2 P[K + 2 * M], Q[K + 2 * M];
 #pragma unroll
-    for (int t = 0; t < K + 2 * A; t++) {
-      P[t] = su[(r0 - A + t + M) * R::RC + (c + b + M)];
-      Q[t] = (b == 0) ? P[t] : su[(r0 - A + t + M) * R::RC + (c - b + M)];
-    }
+    for (int a = -A; a <= A; a++) {
+      if (b == 0 && a <= 0) continue;
+      const int j = sten_index(M, a, b);
+      const double cx = SC<M>(5, j), cy = SC<M>(6, j);
 #pragma unroll
-    for (int k = 0; k < K; k++)
-#pragma unroll
-      for (int a = -A; a <= A; a++) {
-        if (b == 0 && a <= 0) continue;
-        const int j = sten_index(M, a, b);
-        const double2 up = P[k + A + a], um = Q[k + A - a];
-        s0[k] = fma(SC<M>(5, j), up.x - um.x, s0[k]);
-        s1[k] = fma(SC<M>(6, j), up.y - um.y, s1[k]);
+      for (int k = 0; k < 2; k++) {
+        const int r = r0 + k;
+        const double2 up = su[QI<M>(r + a, c + b)], um = su[QI<M>(r - a, c - b)];
+        double dx = up.x - um.x, dy = up.y - um.y;
+        if (!FULL) {
+          // absent neighbours hold u = 0; restore the -u_i of the present side
+          const double mp = (sty[(r + a + M) * R::RT + c + b + M] & kExists) ? 1.0 : 0.0;
+          const double mm = (sty[(r - a + M) * R::RT + c - b + M] & kExists) ? 1.0 : 0.0;
+          const double2 ui = k == 0 ? ui0 : ui1;
+          dx = fma(mm - mp, ui.x, dx);
+          dy = fma(mm - mp, ui.y, dy);
+        }
+        if (k == 0) {
+          s00 = fma(cx, dx, s00);
+          s01 = fma(cy, dy, s01);
+        } else {
+          s10 = fma(cx, dx, s10);
+          s11 = fma(cy, dy, s11);
+        }
       }
-  }
-}
-
-template <int M>
-__device__ __forceinline__ double theta_cell_masked(const double2 *__restrict__ su, const uint8_t *__restrict__ sty,
-                                                    int r, int c) {
-  using R = Region<M>;
-  constexpr Sten<M> S = make_sten<M>();
-  const double2 ui = su[(r + M) * R::RC + (c + M)];
-  double s0 = 0.0, s1 = 0.0;
-#pragma unroll
-  for (int j = 0; j < Sten<M>::N; j++) {
-    const int rr = r + M + S.a[j], cc = c + M + S.b[j];
-    if (sty[rr * R::RT + cc] & kExists) {
-      const double2 uj = su[rr * R::RC + cc];
-      s0 = fma(SC<M>(5, j), uj.x - ui.x, s0);
-      s1 = fma(SC<M>(6, j), uj.y - ui.y, s1);
     }
   }
-  return s0 + s1;
+  th[0] = s00 + s01;
+  th[1] = s10 + s11;
 }
 
+template <int M, bool FULL>
+__device__ __forceinline__ void force_tile(const double2 *__restrict__ su, const double2 *__restrict__ sab, int r0,
+                                           int c, double2 F[2]) {
+  double2 ui[2], ab_i[2];
+  double F0[2] = {0.0, 0.0}, F1[2] = {0.0, 0.0};
+#pragma unroll
+  for (int k = 0; k < 2; k++) {
+    ui[k] = su[QI<M>(r0 + k, c)];
+    ab_i[k] = sab[QI<M>(r0 + k, c)];
+  }
+#pragma unroll
+  for (int b = 0; b <= M; b++) {
+    const int A = amax(M, b);
+#pragma unroll
+    for (int a = -A; a <= A; a++) {
+      if (b == 0 && a <= 0) continue;
+      const int j = sten_index(M, a, b);
+      const double hx = SC<M>(0, j), hy = SC<M>(1, j), L = SC<M>(2, j);
+      const double gx = SC<M>(3, j), gy = SC<M>(4, j);
+#pragma unroll
+      for (int k = 0; k < 2; k++) {
+        const int r = r0 + k;
+        const int qp = QI<M>(r + a, c + b), qm = QI<M>(r - a, c - b);
+        const double2 up = su[qp], um = su[qm], abp = sab[qp], abm = sab[qm];
+        const double e1 = hx * (up.x - ui[k].x) + hy * (up.y - ui[k].y);
+        const double e2 = hx * (ui[k].x - um.x) + hy * (ui[k].y - um.y);
+        double T, wp, wm;
+        if (FULL) {
+          T = (abp.x - abm.x) * L;
+          wp = ab_i[k].y + abp.y;
+          wm = ab_i[k].y + abm.y;
+        } else {
+          // a valid neighbour has B > 0; an absent one has A = B = 0
+          const double mp = abp.y > 0.0 ? 1.0 : 0.0, mm = abm.y > 0.0 ? 1.0 : 0.0;
+          T = fma(mp - mm, ab_i[k].x, abp.x - abm.x) * L;
+          wp = fma(mp, ab_i[k].y, abp.y);
+          wm = fma(mm, ab_i[k].y, abm.y);
+        }
+        T = fma(wp, e1, T);
+        T = fma(-wm, e2, T);
+        F0[k] = fma(T, gx, F0[k]);
+        F1[k] = fma(T, gy, F1[k]);
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 2; k++) F[k] = make_double2(F0[k], F1[k]);
+}
+
+// ---------------------------------------------------------------------------
+// Predicted displacements -> dilatation, persistent over tiles.
 template <int M>
-__global__ void __launch_bounds__(kTileThreads)
+__global__ void __launch_bounds__(kTileThreads, 2)
     k_theta_tma(const __grid_constant__ CUtensorMap map_u, const __grid_constant__ CUtensorMap map_type, Geo g,
                 const DenseTile *__restrict__ tiles, int tile_begin, int n_tiles, StepPtrs p, int pitch,
                 int skip_abc, int *err) {
@@ -305,12 +363,10 @@ __global__ void __launch_bounds__(kTileThreads)
     const InstParams &P = c_inst[t.inst];
     double2 *su = reinterpret_cast<double2 *>(smem + stage * R::THETA_STAGE);
     uint8_t *sty = reinterpret_cast<uint8_t *>(smem + stage * R::THETA_STAGE + R::T_TY);
-    const int r0 = warp * kCellsPerThread;
+    const int r0 = 2 * warp;
     // m_i of the owned cells, fetched while the copy lands
-    double mi[kCellsPerThread];
-#pragma unroll
-    for (int k = 0; k < kCellsPerThread; k++)
-      mi[k] = g.m[(size_t)(t.row + M + r0 + k) * pitch + t.col + M + lane];
+    const size_t cell0 = (size_t)(t.row + M + r0) * pitch + t.col + M + lane;
+    const double mi0 = g.m[cell0], mi1 = g.m[cell0 + pitch];
     if (!mbar_wait_bounded(&bar[stage], (it >> 1) & 1, err)) return;
     if (t.flags & kTileAbc) {
       // ABC nodes: u^n from the last G_u, predicted here (src/main.cpp:727)
@@ -333,30 +389,18 @@ __global__ void __launch_bounds__(kTileThreads)
       }
       __syncthreads();
     }
-    double th[kCellsPerThread];
-    if (t.flags & kTileFull) {
-      double2 ui[kCellsPerThread];
-      double s0[kCellsPerThread], s1[kCellsPerThread];
+    double th[2];
+    if (t.flags & kTileFull)
+      theta_tile<M, true>(su, sty, r0, lane, th);
+    else
+      theta_tile<M, false>(su, sty, r0, lane, th);
 #pragma unroll
-      for (int k = 0; k < kCellsPerThread; k++) {
-        s0[k] = s1[k] = 0.0;
-        ui[k] = su[(r0 + k + M) * R::RC + lane + M];
-      }
-      theta_tile_full<M>(su, lane, r0, ui, s0, s1);
-#pragma unroll
-      for (int k = 0; k < kCellsPerThread; k++) th[k] = s0[k] + s1[k];
-    } else {
-#pragma unroll 1
-      for (int k = 0; k < kCellsPerThread; k++)
-        th[k] = (sty[(r0 + k + M) * R::RT + lane + M] & kExists) ? theta_cell_masked<M>(su, sty, r0 + k, lane) : 0.0;
-    }
-#pragma unroll
-    for (int k = 0; k < kCellsPerThread; k++) {
+    for (int k = 0; k < 2; k++) {
       const uint8_t ty = sty[(r0 + k + M) * R::RT + lane + M];
       if (!(ty & kExists)) continue;
       if (skip_abc && (ty & kActiveAbc)) continue;  // the G_theta kernel writes it
-      const size_t cell = (size_t)(t.row + M + r0 + k) * pitch + t.col + M + lane;
-      p.th_np1[cell] = (mi[k] > 0.0) ? (2.0 / mi[k]) * th[k] : 0.0;
+      const double mi = k == 0 ? mi0 : mi1;
+      p.th_np1[cell0 + (size_t)k * pitch] = (mi > 0.0) ? (2.0 / mi) * th[k] : 0.0;
     }
     fence_proxy_async_smem();
     __syncthreads();  // the stage is refilled at the start of the next-but-one iteration
@@ -365,85 +409,10 @@ __global__ void __launch_bounds__(kTileThreads)
 
 // ---------------------------------------------------------------------------
 // Force + corrector + next predictor, persistent over tiles.  After the copy
-// lands, theta is turned into A = 2(l-m)/m theta in place and invalid
-// neighbours (m <= 0, src/main.cpp:852) get A = B = 0 and a cleared bit.
-constexpr uint8_t kForceValid = 0x80;
-
+// lands, (theta, coef) become (A, B) = (2(l-m)/m theta, 8 mu/m) in the coef
+// slot; absent neighbours and m <= 0 (src/main.cpp:852) get A = B = 0.
 template <int M>
-__device__ __forceinline__ void force_tile_full(const double2 *__restrict__ su, const double *__restrict__ sA,
-                                                const double2 *__restrict__ sco, int lane, int r0, const double2 ui[4],
-                                                const double Bi[4], double F0[4], double F1[4]) {
-  using R = Region<M>;
-  const int c = lane;
-#pragma unroll
-  for (int b = 0; b <= M; b++) {
-    constexpr int K = kCellsPerThread;
-    const int A = amax(M, b);
-    double2 Pu[K + 2 * M], Qu[K + 2 * M];
-    double PA[K + 2 * M], QA[K + 2 * M], PB[K + 2 * M], QB[K + 2 * M];
-#pragma unroll
-    for (int t = 0; t < K + 2 * A; t++) {
-      const int qp = (r0 - A + t + M) * R::RC + (c + b + M);
-      Pu[t] = su[qp];
-      PA[t] = sA[qp];
-      PB[t] = sco[qp].y;
-      if (b == 0) {
-        Qu[t] = Pu[t];
-        QA[t] = PA[t];
-        QB[t] = PB[t];
-      } else {
-        const int qm = (r0 - A + t + M) * R::RC + (c - b + M);
-        Qu[t] = su[qm];
-        QA[t] = sA[qm];
-        QB[t] = sco[qm].y;
-      }
-    }
-#pragma unroll
-    for (int k = 0; k < K; k++)
-#pragma unroll
-      for (int a = -A; a <= A; a++) {
-        if (b == 0 && a <= 0) continue;
-        const int j = sten_index(M, a, b);
-        const double2 up = Pu[k + A + a], um = Qu[k + A - a];
-        // pair (a, b) / (-a, -b): f = g [ (A+ - A-) L + (B_i + B+) e+ - (B_i + B-) e- ]
-        const double e1 = SC<M>(0, j) * (up.x - ui[k].x) + SC<M>(1, j) * (up.y - ui[k].y);
-        const double e2 = SC<M>(0, j) * (ui[k].x - um.x) + SC<M>(1, j) * (ui[k].y - um.y);
-        double T = (PA[k + A + a] - QA[k + A - a]) * SC<M>(2, j);
-        T = fma(Bi[k] + PB[k + A + a], e1, T);
-        T = fma(-(Bi[k] + QB[k + A - a]), e2, T);
-        F0[k] = fma(T, SC<M>(3, j), F0[k]);
-        F1[k] = fma(T, SC<M>(4, j), F1[k]);
-      }
-  }
-}
-
-template <int M>
-__device__ __forceinline__ double2 force_cell_masked(const double2 *__restrict__ su, const double *__restrict__ sA,
-                                                     const double2 *__restrict__ sco, const uint8_t *__restrict__ sty,
-                                                     int r, int c) {
-  using R = Region<M>;
-  constexpr Sten<M> S = make_sten<M>();
-  const int q0 = (r + M) * R::RC + (c + M);
-  const double2 ui = su[q0];
-  const double Ai = sA[q0], Bi = sco[q0].y;
-  double F0 = 0.0, F1 = 0.0;
-#pragma unroll
-  for (int j = 0; j < Sten<M>::N; j++) {
-    const int rr = r + M + S.a[j], cc = c + M + S.b[j];
-    if (sty[rr * R::RT + cc] & kForceValid) {
-      const int q = rr * R::RC + cc;
-      const double2 uj = su[q];
-      const double e = SC<M>(0, j) * (uj.x - ui.x) + SC<M>(1, j) * (uj.y - ui.y);
-      const double T = (Ai + sA[q]) * SC<M>(2, j) + (Bi + sco[q].y) * e;
-      F0 = fma(T, SC<M>(3, j), F0);
-      F1 = fma(T, SC<M>(4, j), F1);
-    }
-  }
-  return make_double2(F0, F1);
-}
-
-template <int M>
-__global__ void __launch_bounds__(kTileThreads)
+__global__ void __launch_bounds__(kTileThreads, 2)
     k_force_tma(const __grid_constant__ CUtensorMap map_u, const __grid_constant__ CUtensorMap map_th,
                 const __grid_constant__ CUtensorMap map_coef, const __grid_constant__ CUtensorMap map_type, Geo g,
                 const DenseTile *__restrict__ tiles, int tile_begin, int n_tiles, StepPtrs p, int pitch, int abc_on,
@@ -478,69 +447,43 @@ __global__ void __launch_bounds__(kTileThreads)
     const InstParams &P = c_inst[t.inst];
     unsigned char *base = smem + stage * R::FORCE_STAGE;
     double2 *su = reinterpret_cast<double2 *>(base);
-    double *sA = reinterpret_cast<double *>(base + R::F_TH);
-    double2 *sco = reinterpret_cast<double2 *>(base + R::F_CO);
-    uint8_t *sty = reinterpret_cast<uint8_t *>(base + R::F_TY);
-    const int r0 = warp * kCellsPerThread;
+    const double *sth = reinterpret_cast<const double *>(base + R::F_TH);
+    double2 *sab = reinterpret_cast<double2 *>(base + R::F_CO);
+    const uint8_t *sty = reinterpret_cast<const uint8_t *>(base + R::F_TY);
+    const int r0 = 2 * warp;
     // corrector inputs of the owned cells, fetched while the copy lands
-    double2 vh[kCellsPerThread];
-#pragma unroll
-    for (int k = 0; k < kCellsPerThread; k++)
-      vh[k] = p.vh[(size_t)(t.row + M + r0 + k) * pitch + t.col + M + lane];
+    const size_t cell0 = (size_t)(t.row + M + r0) * pitch + t.col + M + lane;
+    const double2 vh0 = p.vh[cell0], vh1 = p.vh[cell0 + pitch];
     if (!mbar_wait_bounded(&bar[stage], (it >> 1) & 1, err)) return;
-    // theta -> A = 2(l - m)/m_j theta_j; validity bit
     for (int q = tid; q < R::CELLS; q += kTileThreads) {
       const int rr = q / R::RC, cc = q - rr * R::RC;
-      const double2 co = sco[q];
-      uint8_t ty = sty[rr * R::RT + cc];
-      if ((ty & kExists) && co.y >= 0.0) {
-        sA[q] = co.x * sA[q];
-        ty |= kForceValid;
-      } else {
-        sA[q] = 0.0;
-        sco[q] = make_double2(0.0, 0.0);
-      }
-      sty[rr * R::RT + cc] = ty;
+      const double2 co = sab[q];
+      const bool valid = (sty[rr * R::RT + cc] & kExists) && co.y >= 0.0;
+      sab[q] = valid ? make_double2(co.x * sth[q], co.y) : make_double2(0.0, 0.0);
     }
     __syncthreads();
-    double2 acc[kCellsPerThread];
-    if (t.flags & kTileFull) {
-      double2 ui[kCellsPerThread];
-      double Bi[kCellsPerThread], F0[kCellsPerThread], F1[kCellsPerThread];
+    double2 F[2];
+    if (t.flags & kTileFull)
+      force_tile<M, true>(su, sab, r0, lane, F);
+    else
+      force_tile<M, false>(su, sab, r0, lane, F);
 #pragma unroll
-      for (int k = 0; k < kCellsPerThread; k++) {
-        const int q0 = (r0 + k + M) * R::RC + lane + M;
-        ui[k] = su[q0];
-        Bi[k] = sco[q0].y;
-        F0[k] = F1[k] = 0.0;
-      }
-      force_tile_full<M>(su, sA, sco, lane, r0, ui, Bi, F0, F1);
-#pragma unroll
-      for (int k = 0; k < kCellsPerThread; k++) acc[k] = make_double2(F0[k] / P.rho, F1[k] / P.rho);
-    } else {
-#pragma unroll 1
-      for (int k = 0; k < kCellsPerThread; k++) {
-        acc[k] = make_double2(0.0, 0.0);
-        if (sty[(r0 + k + M) * R::RT + lane + M] & kForceValid) {
-          const double2 F = force_cell_masked<M>(su, sA, sco, sty, r0 + k, lane);
-          acc[k] = make_double2(F.x / P.rho, F.y / P.rho);
-        }
-      }
-    }
-#pragma unroll
-    for (int k = 0; k < kCellsPerThread; k++) {
+    for (int k = 0; k < 2; k++) {
       const uint8_t ty = sty[(r0 + k + M) * R::RT + lane + M];
       if (!(ty & kExists)) continue;
-      const size_t cell = (size_t)(t.row + M + r0 + k) * pitch + t.col + M + lane;
-      p.a_np1[cell] = acc[k];
+      const size_t cell = cell0 + (size_t)k * pitch;
+      const bool valid = sab[QI<M>(r0 + k, lane)].y > 0.0;  // m_i > 0 (:827-831)
+      const double2 acc = valid ? make_double2(F[k].x / P.rho, F[k].y / P.rho) : make_double2(0.0, 0.0);
+      p.a_np1[cell] = acc;
       if (abc_on && (ty & kActiveAbc)) continue;  // G_v writes v; the next theta kernel predicts u
       // corrector (:924) then the next predictor (:727) from the same values
+      const double2 vh = k == 0 ? vh0 : vh1;
       double2 v, vh2, un;
-      v.x = vh[k].x + P.half_dt * acc[k].x;
-      v.y = vh[k].y + P.half_dt * acc[k].y;
-      vh2.x = v.x + P.half_dt * acc[k].x;
-      vh2.y = v.y + P.half_dt * acc[k].y;
-      const double2 u = su[(r0 + k + M) * R::RC + lane + M];
+      v.x = vh.x + P.half_dt * acc.x;
+      v.y = vh.y + P.half_dt * acc.y;
+      vh2.x = v.x + P.half_dt * acc.x;
+      vh2.y = v.y + P.half_dt * acc.y;
+      const double2 u = su[QI<M>(r0 + k, lane)];
       un.x = u.x + P.dt * vh2.x;
       un.y = u.y + P.dt * vh2.y;
       p.v_np1[cell] = v;
