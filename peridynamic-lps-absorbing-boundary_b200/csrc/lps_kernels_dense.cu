@@ -743,20 +743,27 @@ int enqueue_dense_step(const DenseGeo &dg, const LaunchGeo &lg, const StepPtrs &
   const bool abc = lg.abcs_step != -1 && lg.abc.n_abc > 0;
   const bool gth = abc && lg.theta_method == 1;
   const int rth = p.th_ring;
+  // With a timing mark the absorbing-boundary kernels run on the main stream
+  // (serialised), so each kernel's device time can be read between events.
+  const bool fork = mark == nullptr;
+  cudaStream_t side = fork ? dg.side : st;
   // pass 1: theta tiles || G_theta
   if (gth) {
-    cudaEventRecord(dg.ev_fork[0], st);
-    cudaStreamWaitEvent(dg.side, dg.ev_fork[0], 0);
-    k_abc_theta<<<lg.n_abc_blocks, 256, 0, dg.side>>>(lg.abc, p.th_n, p.th_nm1, p.th_np1);
-    cudaEventRecord(dg.ev_join[0], dg.side);
+    if (fork) {
+      cudaEventRecord(dg.ev_fork[0], st);
+      cudaStreamWaitEvent(side, dg.ev_fork[0], 0);
+    }
+    k_abc_theta<<<lg.n_abc_blocks, 256, 0, side>>>(lg.abc, p.th_n, p.th_nm1, p.th_np1);
+    if (fork) cudaEventRecord(dg.ev_join[0], side);
+    if (mark) (*mark)("abc_theta");
     k++;
   }
   for (const auto &gr : dg.groups) {
     LPS_DISPATCH_M(gr.m, launch_theta_group, gr, lg, dg, p, ring_u, gth, st);
     k++;
   }
-  if (gth) cudaStreamWaitEvent(st, dg.ev_join[0], 0);
-  if (mark) (*mark)("theta_dense");
+  if (gth && fork) cudaStreamWaitEvent(st, dg.ev_join[0], 0);
+  if (mark) (*mark)("theta_tiles");
   if (abc && lg.theta_method == 0) {
     launch_theta_idw(lg, p.th_np1, st);
     if (mark) (*mark)("theta_idw");
@@ -764,10 +771,13 @@ int enqueue_dense_step(const DenseGeo &dg, const LaunchGeo &lg, const StepPtrs &
   }
   // pass 2: force tiles || G_u, G_v
   if (abc) {
-    cudaEventRecord(dg.ev_fork[1], st);
-    cudaStreamWaitEvent(dg.side, dg.ev_fork[1], 0);
-    k_abc_uv<<<lg.n_abc_blocks, 256, 0, dg.side>>>(lg.abc, p);
-    cudaEventRecord(dg.ev_join[1], dg.side);
+    if (fork) {
+      cudaEventRecord(dg.ev_fork[1], st);
+      cudaStreamWaitEvent(side, dg.ev_fork[1], 0);
+    }
+    k_abc_uv<<<lg.n_abc_blocks, 256, 0, side>>>(lg.abc, p);
+    if (fork) cudaEventRecord(dg.ev_join[1], side);
+    if (mark) (*mark)("abc_uv");
     k++;
   }
   bool first = true;
@@ -776,8 +786,8 @@ int enqueue_dense_step(const DenseGeo &dg, const LaunchGeo &lg, const StepPtrs &
     first = false;
     k++;
   }
-  if (abc) cudaStreamWaitEvent(st, dg.ev_join[1], 0);
-  if (mark) (*mark)("force_dense");
+  if (abc && fork) cudaStreamWaitEvent(st, dg.ev_join[1], 0);
+  if (mark) (*mark)("force_tiles");
   return k;
 }
 
