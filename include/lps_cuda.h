@@ -181,6 +181,33 @@ typedef struct lps_kernel_time {
 int lps_profile_kernels(lps_handle *h, int n_steps, int diag_every, lps_kernel_time *out,
                         int max_kinds, int *n_kinds);
 
+/* State diagnostics without any allocation.  No counterpart in the
+ * reference: it exists for callers that must not allocate device memory when
+ * they call it (a time-critical loop that cannot afford cudaMalloc's implicit
+ * synchronisation, a host whose GPU memory is owned by another allocator, code
+ * running during a stream capture).  Given one instance's state already in
+ * device memory -- xy, u, v, a as [2N] x/y interleaved doubles, theta [N] --
+ * it enqueues on `stream` (NULL: the legacy default stream) the kinetic
+ * energy, momentum and maxima of an output step, src/main.cpp:992-1016
+ * (energy and momentum over r <= exclude_r when exclude_r > 0), and writes
+ * LPS_NOALLOC_OUT doubles to the device buffer `out`:
+ *   Ek, Px, Py, max|u|, max|v|, max|a|, theta_min, theta_max,
+ *   node of max|u|, node of max|v|   (-1 when every magnitude is 0).
+ * Its scratch is a file-scope device array sized for LPS_NOALLOC_MAX_NODES
+ * nodes (about 0.46 MB on every GPU that loads the library, held until the
+ * process exits); larger n_nodes is rejected with LPS_ERR_INVALID_ARG and a
+ * message in lps_last_error(NULL).  The first call on a device resolves the
+ * array's device address (cudaGetSymbolAddress) -- make that first call before
+ * any stream capture on the device.  All calls on a device share the array,
+ * so calls that overlap on the GPU (different streams, no ordering) race;
+ * every call rewrites the slots it reads, so nothing needs clearing.  The call
+ * returns without synchronising. */
+#define LPS_NOALLOC_MAX_NODES 1048576
+#define LPS_NOALLOC_OUT 10
+int lps_state_diag_noalloc(int n_nodes, const double *xy, const double *u, const double *v,
+                           const double *a, const double *theta, double rho, double dx, double dy,
+                           double exclude_r, double *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -27,6 +27,11 @@ struct DevBuf {
 
 }  // namespace
 
+namespace lps {
+// Error text for entry points that have no handle (read by lps_last_error(NULL)).
+void set_create_error(const char *msg) { g_create_error = msg; }
+}  // namespace lps
+
 struct lps_handle {
   lps_options opt{};
   int n_inst = 0;
