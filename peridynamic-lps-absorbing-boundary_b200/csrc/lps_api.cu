@@ -58,6 +58,7 @@ struct lps_handle {
 
   // state
   double2 *U[kUring] = {}, *V[3] = {}, *A[2] = {}, *VH = nullptr, *S = nullptr;
+  double2 *S1 = nullptr;      // dense path: second G_u result buffer (step parity)
   int ring_u = 3;             // displacement ring depth: 3 (CSR path) or 4 (dense path)
   double *TH[3] = {};
   double2 *U0 = nullptr, *V0 = nullptr;
@@ -228,13 +229,19 @@ void fill_params(InstParams &P, const lps_problem &p, const lps_options &o, cons
   P.abcs_step = o.abcs_step;
 }
 
-int upload_abc(lps_handle *h, const HostAbc &H, int total_abc) {
+int upload_abc(lps_handle *h, const HostAbc &H, int total_abc, const std::vector<int> &abc_of) {
   Abc &B = h->lg.abc;
   int s;
-  int *a_node, *a_inst, *a_cl_off, *a_cl_len, *a_cl_idx, *a_idw_off, *a_idw_len, *a_idw_idx;
+  int *a_node, *a_inst, *a_cl_off, *a_cl_len, *a_cl_idx, *a_idw_off, *a_idw_len, *a_idw_idx, *a_cl_src;
   uint8_t *a_writes, *a_active;
   double *a_gu, *a_gv, *a_idw_w;
   double *a_gth;
+  // which cloud entries are themselves G_u-written nodes (their u^n lives in
+  // the previous step's G_u result until the next predictor merges it)
+  std::vector<int> cl_src(H.cl_idx.size());
+  for (size_t e = 0; e < H.cl_idx.size(); e++) cl_src[e] = abc_of[H.cl_idx[e]];
+  if ((s = dev_upload(h, &a_cl_src, cl_src))) return s;
+  B.cl_src = a_cl_src;
   if ((s = dev_upload(h, &a_node, H.node)) || (s = dev_upload(h, &a_inst, H.inst)) ||
       (s = dev_upload(h, &a_cl_off, H.cl_off)) || (s = dev_upload(h, &a_cl_len, H.cl_len)) ||
       (s = dev_upload(h, &a_cl_idx, H.cl_idx)) || (s = dev_upload(h, &a_idw_off, H.idw_off)) ||
@@ -330,7 +337,7 @@ int build_csr(lps_handle *h, const lps_problem *probs) {
     return s;
   G.xy = d_xy; G.coef = d_coef; G.type = d_type; G.abc_of = d_abc_of; G.len = d_len;
   G.nbr = d_nbr; G.blk_inst = d_blk; G.m = d_m;
-  if ((s = upload_abc(h, H, total_abc))) return s;
+  if ((s = upload_abc(h, H, total_abc, abc_of))) return s;
   h->lg.n_node_blocks = total / kNodeBlock;
   h->lg.n_abc_blocks = total_abc / kAbcWarpsPerBlock;
   h->lg.n_inst = K;
@@ -575,7 +582,7 @@ int build_dense(lps_handle *h, const lps_problem *probs, const std::vector<Latti
   G.xy = d_xy; G.coef = d_coef; G.type = d_type; G.abc_of = d_abc_of; G.blk_inst = d_blk; G.m = d_m;
   G.len = nullptr; G.nbr = nullptr;
   D.tiles = d_tiles;
-  if ((st = upload_abc(h, H, total_abc))) return st;
+  if ((st = upload_abc(h, H, total_abc, abc_of))) return st;
   std::map<int, int> done;
   for (int k = 0; k < K; k++) {
     if (done.count(lat[k].M)) continue;
@@ -634,7 +641,15 @@ StepPtrs step_ptrs(lps_handle *h, int64_t n) {
   p.th_n = h->TH[u0];
   p.th_nm1 = h->TH[um];
   p.th_np1 = h->TH[u1];
-  p.s_abc = h->S;
+  if (h->path == LPS_PATH_DENSE) {
+    // the dense step computes G_u concurrently with the predictor that still
+    // reads the previous result, so the two alternate by step parity
+    p.s_abc = (n + 1) % 2 ? h->S1 : h->S;
+    p.s_prev = n % 2 ? h->S1 : h->S;
+  } else {
+    p.s_abc = h->S;
+    p.s_prev = h->S;
+  }
   return p;
 }
 
@@ -667,7 +682,7 @@ int enqueue_step(lps_handle *h, int64_t n, bool diag, const Mark *mark = nullptr
   if (diag) {
     const bool abc = h->opt.abcs_step != -1 && h->lg.abc.n_abc > 0;
     if (abc) {
-      launch_merge_abc(h->lg, p.u_np1, h->S, st);
+      launch_merge_abc(h->lg, p.u_np1, p.s_abc, st);
       M("merge_abc");
       k++;
     }
@@ -805,6 +820,7 @@ int alloc_state(lps_handle *h) {
     LPS_CUDA_TRY(h, cudaMemset(h->A[r], 0, sizeof(double2) * n));
   }
   if ((s = dev_alloc(h, &h->VH, n)) || (s = dev_alloc(h, &h->S, std::max(h->n_abc_total, 1))) ||
+      (s = dev_alloc(h, &h->S1, std::max(h->n_abc_total, 1))) ||
       (s = dev_alloc(h, &h->U0, n)) || (s = dev_alloc(h, &h->V0, n)))
     return s;
   LPS_CUDA_TRY(h, cudaMemset(h->VH, 0, sizeof(double2) * n));
@@ -1099,7 +1115,8 @@ int lps_download(lps_handle *h, int instance, double *u, double *v, double *a, d
   const int64_t n = h->step;
   // the newest level: after step n the current level is n
   const int cur = (int)(n % h->ring_u), cur3 = (int)(n % 3), cura = (int)(n % 2);
-  if (h->opt.abcs_step != -1 && h->lg.abc.n_abc > 0) launch_merge_abc(h->lg, h->U[cur], h->S, h->stream);
+  if (h->opt.abcs_step != -1 && h->lg.abc.n_abc > 0)
+    launch_merge_abc(h->lg, h->U[cur], (h->path == LPS_PATH_DENSE && n % 2) ? h->S1 : h->S, h->stream);
   LPS_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   if (int e = check_device_error(h)) return e;
   const int nn = h->node_count[instance];

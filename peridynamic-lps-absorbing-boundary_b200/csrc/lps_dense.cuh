@@ -66,6 +66,7 @@ struct DenseGeo {
   std::vector<DenseGroup> groups;
   int pitch = 0;
   int total_rows = 0;
+  int tile_priority = 0;                       // launch priority of the tile kernels
   cudaStream_t side = nullptr;                 // forked stream for the ABC kernels
   cudaEvent_t ev_fork[2] = {nullptr, nullptr}, ev_join[2] = {nullptr, nullptr};
   int *d_err = nullptr;                        // device wait-timeout flag

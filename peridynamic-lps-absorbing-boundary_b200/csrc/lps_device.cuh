@@ -68,6 +68,7 @@ struct StepPtrs {
   double *th_np1;
   double2 *s_abc;          // G_u result u^{n+1} at ABC nodes, merged next step
   double2 *u_np2;          // dense path: predicted u^{n+2}, written by the force pass
+  const double2 *s_prev;   // dense path: G_u result of the previous step (u^n at ABC nodes)
   int th_ring;             // ring index of th_np1
   int pad;
 };
@@ -95,6 +96,7 @@ struct Abc {
   const uint8_t *active;       // BCTypes[2 node] == 1
   const int *cl_off, *cl_len;  // compacted cloud list (k != -1 only)
   const int *cl_idx;           // global node index per cloud entry
+  const int *cl_src;           // per cloud entry: ABC entry whose G_u writes that node, or -1
   const double *gu;            // per entry 8 doubles: row x [4], row y [4]
   const double *gv;            // same
   const double *gth;           // per node: rows theta^n, theta^{n-1} of cl_len weights

@@ -374,7 +374,7 @@ __global__ void __launch_bounds__(kTileThreads, 2)
         const int rr = q / R::RC, cc = q - rr * R::RC;
         if (!(sty[rr * R::RT + cc] & kActiveAbc)) continue;
         const size_t cell = (size_t)(t.row + rr) * pitch + t.col + cc;
-        const double2 u = p.s_abc[g.abc_of[cell]], v = p.v_n[cell], a = p.a_n[cell];
+        const double2 u = p.s_prev[g.abc_of[cell]], v = p.v_n[cell], a = p.a_n[cell];
         double2 vh, up;
         vh.x = v.x + P.half_dt * a.x;
         vh.y = v.y + P.half_dt * a.y;
@@ -505,6 +505,77 @@ __global__ void __launch_bounds__(256) k_abc_theta(Abc ab, const double *th_n, c
 __global__ void __launch_bounds__(256) k_abc_uv(Abc ab, StepPtrs p) {
   const int a = blockIdx.x * kAbcWarpsPerBlock + (threadIdx.x >> 5);
   abc_uv_warp(ab, a, p);
+}
+
+// G_theta (src/main.cpp:795-812), G_u (:883-916) and G_v (:933-974) of one
+// step for one ABC node per warp.  It runs while the tile kernel of the same
+// step is predicting and merging displacements, so u^n of a cloud node that
+// is itself G_u-written comes from the previous step's G_u result
+// (p.s_prev), and the result goes to the other buffer (p.s_abc).  Every
+// lane issues the loads of its two cloud entries before it uses any of them.
+__global__ void __launch_bounds__(256) k_abc_step(Abc ab, StepPtrs p, int do_theta) {
+  const int lane = threadIdx.x & 31;
+  const int a = blockIdx.x * kAbcWarpsPerBlock + (threadIdx.x >> 5);
+  if (a >= ab.n_abc || !ab.writes[a]) return;
+  const InstParams &P = c_inst[ab.inst[a]];
+  const int off = ab.cl_off[a], len = ab.cl_len[a];
+  const double *__restrict__ gu = ab.gu + 8 * (size_t)off;
+  const double *__restrict__ gv = ab.gv + 8 * (size_t)off;
+  const double *__restrict__ gt = ab.gth + 2 * (size_t)off;
+  const bool kin = P.kinematic != 0;
+  double ux = 0.0, uy = 0.0, vx = 0.0, vy = 0.0, th = 0.0;
+  for (int e0 = 0; e0 < len; e0 += 64) {
+    int e[2], k[2], src[2];
+    bool ok[2];
+    double G[2][8], H[2][8], W[2][2];
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      e[q] = e0 + 32 * q + lane;
+      ok[q] = e[q] < len;
+      k[q] = ok[q] ? __ldg(ab.cl_idx + off + e[q]) : 0;
+      src[q] = ok[q] ? __ldg(ab.cl_src + off + e[q]) : -1;
+#pragma unroll
+      for (int r = 0; r < 8; r++) {
+        G[q][r] = ok[q] ? __ldg(gu + r * len + e[q]) : 0.0;
+        H[q][r] = (ok[q] && !kin) ? __ldg(gv + r * len + e[q]) : 0.0;
+      }
+      W[q][0] = (ok[q] && do_theta) ? __ldg(gt + e[q]) : 0.0;
+      W[q][1] = (ok[q] && do_theta) ? __ldg(gt + len + e[q]) : 0.0;
+    }
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      if (!ok[q]) continue;
+      const double2 un = src[q] >= 0 ? p.s_prev[src[q]] : p.u_n[k[q]];
+      const double2 um = p.u_nm1[k[q]];
+      ux += G[q][0] * un.x + G[q][1] * un.y + G[q][2] * um.x + G[q][3] * um.y;
+      uy += G[q][4] * un.x + G[q][5] * un.y + G[q][6] * um.x + G[q][7] * um.y;
+      if (!kin) {
+        const double2 vn = p.v_n[k[q]], vm = p.v_nm1[k[q]];
+        vx += H[q][0] * vn.x + H[q][1] * vn.y + H[q][2] * vm.x + H[q][3] * vm.y;
+        vy += H[q][4] * vn.x + H[q][5] * vn.y + H[q][6] * vm.x + H[q][7] * vm.y;
+      }
+      if (do_theta) th += W[q][0] * p.th_n[k[q]] + W[q][1] * p.th_nm1[k[q]];
+    }
+  }
+  ux = warp_sum(ux);
+  uy = warp_sum(uy);
+  if (!kin) {
+    vx = warp_sum(vx);
+    vy = warp_sum(vy);
+  }
+  if (do_theta) th = warp_sum(th);
+  if (lane == 0) {
+    const int node = ab.node[a];
+    p.s_abc[a] = make_double2(ux, uy);
+    if (kin) {
+      // v = (u^{n+1} - u^n) / dt with this node's u^n, src/main.cpp:940-943
+      const double2 un = p.s_prev[a];
+      p.v_np1[node] = make_double2((ux - un.x) / P.dt, (uy - un.y) / P.dt);
+    } else {
+      p.v_np1[node] = make_double2(vx, vy);
+    }
+    if (do_theta) p.th_np1[node] = th;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -645,7 +716,9 @@ static cudaError_t prepare_m(DenseGroup &gr, int n_sm) {
     return e;
   bt = std::max(bt, 1);
   bf = std::max(bf, 1);
-  gr.grid_theta = std::min(gr.n_tiles, bt * n_sm);
+  // at most 2 theta CTAs per SM: the rest of the SM runs the concurrent
+  // absorbing-boundary kernel of the same step
+  gr.grid_theta = std::min(gr.n_tiles, std::min(bt, 2) * n_sm);
   gr.grid_force = std::min(gr.n_tiles, bf * n_sm);
   return cudaSuccess;
 }
@@ -656,9 +729,11 @@ static void prepare_dispatch(DenseGroup &gr, int n_sm, cudaError_t *e) {
 }
 
 cudaError_t dense_prepare(DenseGeo &dg) {
-  int dev = 0, n_sm = 0;
+  int dev = 0, n_sm = 0, least = 0, greatest = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+  cudaDeviceGetStreamPriorityRange(&least, &greatest);
+  dg.tile_priority = greatest;  // tile CTAs are dispatched ahead of the ABC kernel's blocks
   for (auto &gr : dg.groups) {
     cudaError_t e = cudaErrorInvalidValue;
     LPS_DISPATCH_M(gr.m, prepare_dispatch, gr, n_sm, &e);
@@ -722,9 +797,18 @@ int dense_encode_maps(DenseGroup &g, int pitch, int total_rows, double2 *const *
 template <int M>
 static void launch_theta_group(const DenseGroup &gr, const LaunchGeo &lg, const DenseGeo &dg, const StepPtrs &p,
                                int ring_u, bool skip_abc, cudaStream_t st) {
-  k_theta_tma<M><<<gr.grid_theta, kTileThreads, Region<M>::THETA_SMEM, st>>>(
-      gr.maps.u[ring_u], gr.maps.type, lg.geo, dg.tiles, gr.tile_begin, gr.n_tiles, p, dg.pitch, skip_abc ? 1 : 0,
-      dg.d_err);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(gr.grid_theta);
+  cfg.blockDim = dim3(kTileThreads);
+  cfg.dynamicSmemBytes = Region<M>::THETA_SMEM;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributePriority;
+  attr[0].val.priority = dg.tile_priority;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, k_theta_tma<M>, gr.maps.u[ring_u], gr.maps.type, lg.geo, dg.tiles, gr.tile_begin,
+                     gr.n_tiles, p, dg.pitch, skip_abc ? 1 : 0, dg.d_err);
 }
 
 template <int M>
@@ -747,46 +831,35 @@ int enqueue_dense_step(const DenseGeo &dg, const LaunchGeo &lg, const StepPtrs &
   // (serialised), so each kernel's device time can be read between events.
   const bool fork = mark == nullptr;
   cudaStream_t side = fork ? dg.side : st;
-  // pass 1: theta tiles || G_theta
-  if (gth) {
+  // pass 1: G_theta, G_u, G_v of this step || predicted u -> theta tiles
+  if (abc) {
     if (fork) {
       cudaEventRecord(dg.ev_fork[0], st);
       cudaStreamWaitEvent(side, dg.ev_fork[0], 0);
     }
-    k_abc_theta<<<lg.n_abc_blocks, 256, 0, side>>>(lg.abc, p.th_n, p.th_nm1, p.th_np1);
+    k_abc_step<<<lg.n_abc_blocks, 256, 0, side>>>(lg.abc, p, gth ? 1 : 0);
     if (fork) cudaEventRecord(dg.ev_join[0], side);
-    if (mark) (*mark)("abc_theta");
+    if (mark) (*mark)("abc_step");
     k++;
   }
   for (const auto &gr : dg.groups) {
     LPS_DISPATCH_M(gr.m, launch_theta_group, gr, lg, dg, p, ring_u, gth, st);
     k++;
   }
-  if (gth && fork) cudaStreamWaitEvent(st, dg.ev_join[0], 0);
+  if (abc && fork) cudaStreamWaitEvent(st, dg.ev_join[0], 0);
   if (mark) (*mark)("theta_tiles");
   if (abc && lg.theta_method == 0) {
     launch_theta_idw(lg, p.th_np1, st);
     if (mark) (*mark)("theta_idw");
     k++;
   }
-  // pass 2: force tiles || G_u, G_v
-  if (abc) {
-    if (fork) {
-      cudaEventRecord(dg.ev_fork[1], st);
-      cudaStreamWaitEvent(side, dg.ev_fork[1], 0);
-    }
-    k_abc_uv<<<lg.n_abc_blocks, 256, 0, side>>>(lg.abc, p);
-    if (fork) cudaEventRecord(dg.ev_join[1], side);
-    if (mark) (*mark)("abc_uv");
-    k++;
-  }
+  // pass 2: force tiles
   bool first = true;
   for (const auto &gr : dg.groups) {
     LPS_DISPATCH_M(gr.m, launch_force_group, gr, lg, dg, p, ring_u, rth, abc, first, d_step, st);
     first = false;
     k++;
   }
-  if (abc && fork) cudaStreamWaitEvent(st, dg.ev_join[1], 0);
   if (mark) (*mark)("force_tiles");
   return k;
 }
