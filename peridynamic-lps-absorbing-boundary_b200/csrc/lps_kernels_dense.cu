@@ -507,13 +507,12 @@ __global__ void __launch_bounds__(256) k_abc_uv(Abc ab, StepPtrs p) {
   abc_uv_warp(ab, a, p);
 }
 
-// G_theta (src/main.cpp:795-812), G_u (:883-916) and G_v (:933-974) of one
-// step for one ABC node per warp.  It runs while the tile kernel of the same
-// step is predicting and merging displacements, so u^n of a cloud node that
-// is itself G_u-written comes from the previous step's G_u result
-// (p.s_prev), and the result goes to the other buffer (p.s_abc).  Every
-// lane issues the loads of its two cloud entries before it uses any of them.
-__global__ void __launch_bounds__(256) k_abc_step(Abc ab, StepPtrs p, int do_theta) {
+// G_u (src/main.cpp:883-916) and G_v (:933-974) of one step for one ABC node
+// per warp, for the dense path.  It runs while the dilatation tiles of the
+// same step are predicting and merging displacements, so u^n of a cloud node
+// that is itself G_u-written comes from the previous step's G_u result
+// (p.s_prev), and the result goes to the other buffer (p.s_abc).
+__global__ void __launch_bounds__(256) k_abc_uv_dense(Abc ab, StepPtrs p) {
   const int lane = threadIdx.x & 31;
   const int a = blockIdx.x * kAbcWarpsPerBlock + (threadIdx.x >> 5);
   if (a >= ab.n_abc || !ab.writes[a]) return;
@@ -521,40 +520,23 @@ __global__ void __launch_bounds__(256) k_abc_step(Abc ab, StepPtrs p, int do_the
   const int off = ab.cl_off[a], len = ab.cl_len[a];
   const double *__restrict__ gu = ab.gu + 8 * (size_t)off;
   const double *__restrict__ gv = ab.gv + 8 * (size_t)off;
-  const double *__restrict__ gt = ab.gth + 2 * (size_t)off;
   const bool kin = P.kinematic != 0;
-  double ux = 0.0, uy = 0.0, vx = 0.0, vy = 0.0, th = 0.0;
+  double ux = 0.0, uy = 0.0, vx = 0.0, vy = 0.0;
+  const double2 z = make_double2(0.0, 0.0);
   for (int e0 = 0; e0 < len; e0 += 64) {
-    int e[2], k[2], src[2];
-    bool ok[2];
-    double G[2][8], H[2][8], W[2][2];
-#pragma unroll
-    for (int q = 0; q < 2; q++) {
-      e[q] = e0 + 32 * q + lane;
-      ok[q] = e[q] < len;
-      k[q] = ok[q] ? __ldg(ab.cl_idx + off + e[q]) : 0;
-      src[q] = ok[q] ? __ldg(ab.cl_src + off + e[q]) : -1;
-#pragma unroll
-      for (int r = 0; r < 8; r++) {
-        G[q][r] = ok[q] ? __ldg(gu + r * len + e[q]) : 0.0;
-        H[q][r] = (ok[q] && !kin) ? __ldg(gv + r * len + e[q]) : 0.0;
-      }
-      W[q][0] = (ok[q] && do_theta) ? __ldg(gt + e[q]) : 0.0;
-      W[q][1] = (ok[q] && do_theta) ? __ldg(gt + len + e[q]) : 0.0;
-    }
-#pragma unroll
-    for (int q = 0; q < 2; q++) {
-      if (!ok[q]) continue;
-      const double2 un = src[q] >= 0 ? p.s_prev[src[q]] : p.u_n[k[q]];
-      const double2 um = p.u_nm1[k[q]];
-      ux += G[q][0] * un.x + G[q][1] * un.y + G[q][2] * um.x + G[q][3] * um.y;
-      uy += G[q][4] * un.x + G[q][5] * un.y + G[q][6] * um.x + G[q][7] * um.y;
-      if (!kin) {
-        const double2 vn = p.v_n[k[q]], vm = p.v_nm1[k[q]];
-        vx += H[q][0] * vn.x + H[q][1] * vn.y + H[q][2] * vm.x + H[q][3] * vm.y;
-        vy += H[q][4] * vn.x + H[q][5] * vn.y + H[q][6] * vm.x + H[q][7] * vm.y;
-      }
-      if (do_theta) th += W[q][0] * p.th_n[k[q]] + W[q][1] * p.th_nm1[k[q]];
+    const int ea = e0 + lane, eb = e0 + 32 + lane;
+    const bool va = ea < len, vb = eb < len;
+    const int ka = va ? __ldg(ab.cl_idx + off + ea) : 0, kb = vb ? __ldg(ab.cl_idx + off + eb) : 0;
+    const int sa = va ? __ldg(ab.cl_src + off + ea) : -1, sb = vb ? __ldg(ab.cl_src + off + eb) : -1;
+    const double2 una = va ? (sa >= 0 ? p.s_prev[sa] : p.u_n[ka]) : z, uma = va ? p.u_nm1[ka] : z;
+    const double2 unb = vb ? (sb >= 0 ? p.s_prev[sb] : p.u_n[kb]) : z, umb = vb ? p.u_nm1[kb] : z;
+    if (va) g_entry(gu, len, ea, una, uma, ux, uy);
+    if (vb) g_entry(gu, len, eb, unb, umb, ux, uy);
+    if (!kin) {
+      const double2 vna = va ? p.v_n[ka] : z, vma = va ? p.v_nm1[ka] : z;
+      const double2 vnb = vb ? p.v_n[kb] : z, vmb = vb ? p.v_nm1[kb] : z;
+      if (va) g_entry(gv, len, ea, vna, vma, vx, vy);
+      if (vb) g_entry(gv, len, eb, vnb, vmb, vx, vy);
     }
   }
   ux = warp_sum(ux);
@@ -563,7 +545,6 @@ __global__ void __launch_bounds__(256) k_abc_step(Abc ab, StepPtrs p, int do_the
     vx = warp_sum(vx);
     vy = warp_sum(vy);
   }
-  if (do_theta) th = warp_sum(th);
   if (lane == 0) {
     const int node = ab.node[a];
     p.s_abc[a] = make_double2(ux, uy);
@@ -574,7 +555,6 @@ __global__ void __launch_bounds__(256) k_abc_step(Abc ab, StepPtrs p, int do_the
     } else {
       p.v_np1[node] = make_double2(vx, vy);
     }
-    if (do_theta) p.th_np1[node] = th;
   }
 }
 
@@ -837,9 +817,14 @@ int enqueue_dense_step(const DenseGeo &dg, const LaunchGeo &lg, const StepPtrs &
       cudaEventRecord(dg.ev_fork[0], st);
       cudaStreamWaitEvent(side, dg.ev_fork[0], 0);
     }
-    k_abc_step<<<lg.n_abc_blocks, 256, 0, side>>>(lg.abc, p, gth ? 1 : 0);
+    if (gth) {
+      k_abc_theta<<<lg.n_abc_blocks, 256, 0, side>>>(lg.abc, p.th_n, p.th_nm1, p.th_np1);
+      if (mark) (*mark)("abc_theta");
+      k++;
+    }
+    k_abc_uv_dense<<<lg.n_abc_blocks, 256, 0, side>>>(lg.abc, p);
     if (fork) cudaEventRecord(dg.ev_join[0], side);
-    if (mark) (*mark)("abc_step");
+    if (mark) (*mark)("abc_uv");
     k++;
   }
   for (const auto &gr : dg.groups) {
