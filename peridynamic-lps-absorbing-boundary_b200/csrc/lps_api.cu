@@ -165,8 +165,11 @@ void pack_abc(const lps_problem &p, const lps_options &o, const InstanceSetup &s
     std::vector<int> js;
     for (int j = 0; j < C; j++)
       if (p.clouds[(size_t)i * C + j] != -1) js.push_back(j);
-    const int len = (int)js.size();
+    // segments have an even length (a zero-weight entry on the node itself
+    // pads odd clouds) so that every operator row starts 16-byte aligned
+    const int len = (int)js.size() + ((int)js.size() & 1);
     for (int j : js) H.cl_idx.push_back(gmap(p.clouds[(size_t)i * C + j]));
+    if (len > (int)js.size()) H.cl_idx.push_back(gmap(node));
     const double *g0 = p.gu + (size_t)(2 * i) * cols, *g1 = p.gu + (size_t)(2 * i + 1) * cols;
     const double *h0 = p.gv + (size_t)(2 * i) * cols, *h1 = p.gv + (size_t)(2 * i + 1) * cols;
     for (int r = 0; r < 8; r++) {
@@ -175,13 +178,19 @@ void pack_abc(const lps_problem &p, const lps_options &o, const InstanceSetup &s
         H.gu.push_back(c < cpc ? (r < 4 ? g0 : g1)[cpc * j + c] : 0.0);
         H.gv.push_back(c < cpc ? (r < 4 ? h0 : h1)[cpc * j + c] : 0.0);
       }
+      if (len > (int)js.size()) {
+        H.gu.push_back(0.0);
+        H.gv.push_back(0.0);
+      }
     }
-    for (int r = 0; r < 2; r++)
+    for (int r = 0; r < 2; r++) {
       for (int j : js) {
         double w = 0.0;
         if (o.theta_method == 1 && p.gtheta && r < cth) w = p.gtheta[(size_t)i * cth * C + cth * j + r];
         H.gth.push_back(w);
       }
+      if (len > (int)js.size()) H.gth.push_back(0.0);
+    }
     H.cl_len[a] = len;
     // inverse-distance lists, src/main.cpp:775-786
     H.idw_off[a] = (int)H.idw_idx.size();

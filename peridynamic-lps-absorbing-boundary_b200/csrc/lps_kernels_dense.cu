@@ -507,6 +507,73 @@ __global__ void __launch_bounds__(256) k_abc_uv(Abc ab, StepPtrs p) {
   abc_uv_warp(ab, a, p);
 }
 
+// G_theta (src/main.cpp:795-812), G_u (:883-916) and G_v (:933-974) of one
+// step for one ABC node per warp, dense path.  Clouds are padded to an even
+// length, so each lane owns an entry pair and reads every operator row as one
+// aligned double2.  It runs while the dilatation tiles of the same step are
+// predicting and merging displacements: u^n of a cloud node that is itself
+// G_u-written comes from the previous step's G_u result (p.s_prev) and the
+// new result goes to the other buffer (p.s_abc).
+__global__ void __launch_bounds__(256, 3) k_abc_dense(Abc ab, StepPtrs p, int do_theta) {
+  const int lane = threadIdx.x & 31;
+  const int a = blockIdx.x * kAbcWarpsPerBlock + (threadIdx.x >> 5);
+  if (a >= ab.n_abc || !ab.writes[a]) return;
+  const InstParams &P = c_inst[ab.inst[a]];
+  const int off = ab.cl_off[a], hp = ab.cl_len[a] >> 1;  // entry pairs
+  const double2 *__restrict__ gu = reinterpret_cast<const double2 *>(ab.gu + 8 * (size_t)off);
+  const double2 *__restrict__ gv = reinterpret_cast<const double2 *>(ab.gv + 8 * (size_t)off);
+  const double2 *__restrict__ gt = reinterpret_cast<const double2 *>(ab.gth + 2 * (size_t)off);
+  const int2 *__restrict__ idx = reinterpret_cast<const int2 *>(ab.cl_idx + off);
+  const int2 *__restrict__ src = reinterpret_cast<const int2 *>(ab.cl_src + off);
+  const bool kin = P.kinematic != 0;
+  double ux = 0.0, uy = 0.0, vx = 0.0, vy = 0.0, th = 0.0;
+  for (int q = lane; q < hp; q += 32) {
+    const int2 k = __ldg(idx + q), s = __ldg(src + q);
+    const double2 un0 = s.x >= 0 ? p.s_prev[s.x] : p.u_n[k.x], um0 = p.u_nm1[k.x];
+    const double2 un1 = s.y >= 0 ? p.s_prev[s.y] : p.u_n[k.y], um1 = p.u_nm1[k.y];
+    const double xs[4][2] = {{un0.x, un1.x}, {un0.y, un1.y}, {um0.x, um1.x}, {um0.y, um1.y}};
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+      const double2 gx = __ldg(gu + r * hp + q), gy = __ldg(gu + (4 + r) * hp + q);
+      ux += gx.x * xs[r][0] + gx.y * xs[r][1];
+      uy += gy.x * xs[r][0] + gy.y * xs[r][1];
+    }
+    if (!kin) {
+      const double2 vn0 = p.v_n[k.x], vm0 = p.v_nm1[k.x], vn1 = p.v_n[k.y], vm1 = p.v_nm1[k.y];
+      const double ys[4][2] = {{vn0.x, vn1.x}, {vn0.y, vn1.y}, {vm0.x, vm1.x}, {vm0.y, vm1.y}};
+#pragma unroll
+      for (int r = 0; r < 4; r++) {
+        const double2 hx = __ldg(gv + r * hp + q), hy = __ldg(gv + (4 + r) * hp + q);
+        vx += hx.x * ys[r][0] + hx.y * ys[r][1];
+        vy += hy.x * ys[r][0] + hy.y * ys[r][1];
+      }
+    }
+    if (do_theta) {
+      const double2 w0 = __ldg(gt + q), w1 = __ldg(gt + hp + q);
+      th += w0.x * p.th_n[k.x] + w0.y * p.th_n[k.y] + w1.x * p.th_nm1[k.x] + w1.y * p.th_nm1[k.y];
+    }
+  }
+  ux = warp_sum(ux);
+  uy = warp_sum(uy);
+  if (!kin) {
+    vx = warp_sum(vx);
+    vy = warp_sum(vy);
+  }
+  if (do_theta) th = warp_sum(th);
+  if (lane == 0) {
+    const int node = ab.node[a];
+    p.s_abc[a] = make_double2(ux, uy);
+    if (kin) {
+      // v = (u^{n+1} - u^n) / dt with this node's u^n, src/main.cpp:940-943
+      const double2 un = p.s_prev[a];
+      p.v_np1[node] = make_double2((ux - un.x) / P.dt, (uy - un.y) / P.dt);
+    } else {
+      p.v_np1[node] = make_double2(vx, vy);
+    }
+    if (do_theta) p.th_np1[node] = th;
+  }
+}
+
 // G_u (src/main.cpp:883-916) and G_v (:933-974) of one step for one ABC node
 // per warp, for the dense path.  It runs while the dilatation tiles of the
 // same step are predicting and merging displacements, so u^n of a cloud node
@@ -817,14 +884,9 @@ int enqueue_dense_step(const DenseGeo &dg, const LaunchGeo &lg, const StepPtrs &
       cudaEventRecord(dg.ev_fork[0], st);
       cudaStreamWaitEvent(side, dg.ev_fork[0], 0);
     }
-    if (gth) {
-      k_abc_theta<<<lg.n_abc_blocks, 256, 0, side>>>(lg.abc, p.th_n, p.th_nm1, p.th_np1);
-      if (mark) (*mark)("abc_theta");
-      k++;
-    }
-    k_abc_uv_dense<<<lg.n_abc_blocks, 256, 0, side>>>(lg.abc, p);
+    k_abc_dense<<<lg.n_abc_blocks, 256, 0, side>>>(lg.abc, p, gth ? 1 : 0);
     if (fork) cudaEventRecord(dg.ev_join[0], side);
-    if (mark) (*mark)("abc_uv");
+    if (mark) (*mark)("abc_dense");
     k++;
   }
   for (const auto &gr : dg.groups) {
