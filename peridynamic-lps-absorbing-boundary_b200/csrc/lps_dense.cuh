@@ -67,6 +67,7 @@ struct DenseGeo {
   int pitch = 0;
   int total_rows = 0;
   int tile_priority = 0;                       // launch priority of the tile kernels
+  int abc_grid = 1, abc_stage = 0, abc_smem = 0;  // bulk-copy ABC kernel launch shape
   cudaStream_t side = nullptr;                 // forked stream for the ABC kernels
   cudaEvent_t ev_fork[2] = {nullptr, nullptr}, ev_join[2] = {nullptr, nullptr};
   int *d_err = nullptr;                        // device wait-timeout flag
@@ -92,6 +93,8 @@ int dense_encode_maps(DenseGroup &g, int pitch, int total_rows, double2 *const *
                       const double2 *coef, const uint8_t *type, std::string &err);
 // Sets shared-memory limits and the persistent grid sizes of each group.
 cudaError_t dense_prepare(DenseGeo &dg);
+// Launch shape of the bulk-copy absorbing-boundary kernel.
+cudaError_t dense_prepare_abc(const Abc &ab, DenseGeo &dg);
 
 // One time step: theta tiles || G_theta, [IDW], force tiles || G_u/G_v.
 int enqueue_dense_step(const DenseGeo &dg, const LaunchGeo &lg, const StepPtrs &p, int *d_step,

@@ -574,6 +574,115 @@ __global__ void __launch_bounds__(256, 3) k_abc_dense(Abc ab, StepPtrs p, int do
   }
 }
 
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+// The same step of the absorbing boundary as k_abc_dense, persistent over
+// chunks of operator blocks that bulk copies (cp.async.bulk) stream into two
+// shared-memory stages: while the warps of a CTA apply the operators of one
+// chunk (an ABC node per warp, entry pairs per lane, history gathered from
+// global memory), the next chunk is already in flight.  One CTA per SM.
+__global__ void __launch_bounds__(256) k_abc_bulk(Abc ab, StepPtrs p, int do_theta, int stage_bytes, int *err) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem + 2 * stage_bytes);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (*(volatile int *)err) return;
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  auto issue = [&](int stage, int c) {
+    const AbcChunk ch = ab.chunks[c];
+    mbar_expect_tx(&bar[stage], ch.bytes);
+    bulk_load(smem + stage * stage_bytes, ab.blob + ch.off, ch.bytes, &bar[stage]);
+  };
+  int c = blockIdx.x;
+  if (tid == 0 && c < ab.n_chunks) issue(0, c);
+  for (int it = 0; c < ab.n_chunks; it++, c += gridDim.x) {
+    const int stage = it & 1;
+    if (tid == 0 && c + (int)gridDim.x < ab.n_chunks) issue(stage ^ 1, c + gridDim.x);
+    const AbcChunk ch = ab.chunks[c];
+    int4 ent = make_int4(0, 0, 0, 0);
+    if (warp < ch.count) ent = ab.chunk_entries[ch.first + warp];
+    if (!mbar_wait_bounded(&bar[stage], (it >> 1) & 1, err)) return;
+    if (warp < ch.count) {
+      const int a = ent.x, len = ent.y, hp = len >> 1;
+      const unsigned char *blk = smem + stage * stage_bytes + ent.z;
+      const double2 *gu = reinterpret_cast<const double2 *>(blk);
+      const double2 *gv = gu + 4 * len;
+      const double2 *gt = gv + 4 * len;
+      const int2 *idx = reinterpret_cast<const int2 *>(blk + 144 * len);
+      const int2 *src = idx + hp;
+      const InstParams &P = c_inst[ab.inst[a]];
+      const bool kin = P.kinematic != 0;
+      double ux = 0.0, uy = 0.0, vx = 0.0, vy = 0.0, th = 0.0;
+      for (int q = lane; q < hp; q += 32) {
+        const int2 k = idx[q], s = src[q];
+        const double2 un0 = s.x >= 0 ? p.s_prev[s.x] : p.u_n[k.x], um0 = p.u_nm1[k.x];
+        const double2 un1 = s.y >= 0 ? p.s_prev[s.y] : p.u_n[k.y], um1 = p.u_nm1[k.y];
+        const double xs[4][2] = {{un0.x, un1.x}, {un0.y, un1.y}, {um0.x, um1.x}, {um0.y, um1.y}};
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+          const double2 gx = gu[r * hp + q], gy = gu[(4 + r) * hp + q];
+          ux += gx.x * xs[r][0] + gx.y * xs[r][1];
+          uy += gy.x * xs[r][0] + gy.y * xs[r][1];
+        }
+        if (!kin) {
+          const double2 vn0 = p.v_n[k.x], vm0 = p.v_nm1[k.x], vn1 = p.v_n[k.y], vm1 = p.v_nm1[k.y];
+          const double ys[4][2] = {{vn0.x, vn1.x}, {vn0.y, vn1.y}, {vm0.x, vm1.x}, {vm0.y, vm1.y}};
+#pragma unroll
+          for (int r = 0; r < 4; r++) {
+            const double2 hx = gv[r * hp + q], hy = gv[(4 + r) * hp + q];
+            vx += hx.x * ys[r][0] + hx.y * ys[r][1];
+            vy += hy.x * ys[r][0] + hy.y * ys[r][1];
+          }
+        }
+        if (do_theta) {
+          const double2 w0 = gt[q], w1 = gt[hp + q];
+          th += w0.x * p.th_n[k.x] + w0.y * p.th_n[k.y] + w1.x * p.th_nm1[k.x] + w1.y * p.th_nm1[k.y];
+        }
+      }
+      ux = warp_sum(ux);
+      uy = warp_sum(uy);
+      if (!kin) {
+        vx = warp_sum(vx);
+        vy = warp_sum(vy);
+      }
+      if (do_theta) th = warp_sum(th);
+      if (lane == 0) {
+        const int node = ab.node[a];
+        p.s_abc[a] = make_double2(ux, uy);
+        if (kin) {
+          // v = (u^{n+1} - u^n) / dt with this node's u^n, src/main.cpp:940-943
+          const double2 un = p.s_prev[a];
+          p.v_np1[node] = make_double2((ux - un.x) / P.dt, (uy - un.y) / P.dt);
+        } else {
+          p.v_np1[node] = make_double2(vx, vy);
+        }
+        if (do_theta) p.th_np1[node] = th;
+      }
+    }
+    fence_proxy_async_smem();
+    __syncthreads();  // the stage is refilled at the start of the next-but-one iteration
+  }
+}
+
+cudaError_t dense_prepare_abc(const Abc &ab, DenseGeo &dg) {
+  int dev = 0, n_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+  dg.abc_stage = (std::max(ab.max_chunk_bytes, 16) + 127) / 128 * 128;
+  dg.abc_smem = 2 * dg.abc_stage + 64;
+  dg.abc_grid = std::max(1, std::min(ab.n_chunks, n_sm));
+  return cudaFuncSetAttribute(k_abc_bulk, cudaFuncAttributeMaxDynamicSharedMemorySize, dg.abc_smem);
+}
+
 // G_u (src/main.cpp:883-916) and G_v (:933-974) of one step for one ABC node
 // per warp, for the dense path.  It runs while the dilatation tiles of the
 // same step are predicting and merging displacements, so u^n of a cloud node
@@ -884,9 +993,9 @@ int enqueue_dense_step(const DenseGeo &dg, const LaunchGeo &lg, const StepPtrs &
       cudaEventRecord(dg.ev_fork[0], st);
       cudaStreamWaitEvent(side, dg.ev_fork[0], 0);
     }
-    k_abc_dense<<<lg.n_abc_blocks, 256, 0, side>>>(lg.abc, p, gth ? 1 : 0);
+    k_abc_bulk<<<dg.abc_grid, 256, dg.abc_smem, side>>>(lg.abc, p, gth ? 1 : 0, dg.abc_stage, dg.d_err);
     if (fork) cudaEventRecord(dg.ev_join[0], side);
-    if (mark) (*mark)("abc_dense");
+    if (mark) (*mark)("abc_bulk");
     k++;
   }
   for (const auto &gr : dg.groups) {
