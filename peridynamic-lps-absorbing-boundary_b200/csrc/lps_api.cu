@@ -277,6 +277,7 @@ int upload_abc_blob(lps_handle *h, const HostAbc &H, const std::vector<int> &abc
   std::vector<unsigned char> blob;
   std::vector<AbcChunk> chunks;
   std::vector<int4> ents;
+  std::vector<long long> ent_off;
   AbcChunk cur{0, 0, 0, 0, 0};
   int max_bytes = 0;
   auto push_bytes = [&blob](const void *src, size_t n) {
@@ -293,6 +294,7 @@ int upload_abc_blob(lps_handle *h, const HostAbc &H, const std::vector<int> &abc
       cur = AbcChunk{(long long)blob.size(), (int)ents.size(), 0, 0, 0};
     }
     const size_t off = H.cl_off[a];
+    ent_off.push_back((long long)blob.size());
     push_bytes(&H.gu[8 * off], sizeof(double) * 8 * len);
     push_bytes(&H.gv[8 * off], sizeof(double) * 8 * len);
     push_bytes(&H.gth[2 * off], sizeof(double) * 2 * len);
@@ -311,15 +313,18 @@ int upload_abc_blob(lps_handle *h, const HostAbc &H, const std::vector<int> &abc
   unsigned char *d_blob;
   AbcChunk *d_chunks;
   int4 *d_ents;
+  long long *d_ent_off;
   int s;
   if ((s = dev_upload(h, &d_blob, blob)) || (s = dev_upload(h, &d_chunks, chunks)) ||
-      (s = dev_upload(h, &d_ents, ents)))
+      (s = dev_upload(h, &d_ents, ents)) || (s = dev_upload(h, &d_ent_off, ent_off)))
     return s;
   B.blob = d_blob;
   B.chunks = d_chunks;
   B.chunk_entries = d_ents;
+  B.entry_off = d_ent_off;
   B.n_chunks = (int)chunks.size();
   B.max_chunk_bytes = max_bytes;
+  B.n_entries = (int)ents.size();
   return LPS_OK;
 }
 

@@ -109,9 +109,12 @@ struct Abc {
   // blocks that one bulk copy brings into shared memory.
   const unsigned char *blob;
   const struct AbcChunk *chunks;
-  const int4 *chunk_entries;   // (ABC entry, len, byte offset in the chunk, -)
+  const int4 *chunk_entries;   // (ABC entry, len, byte offset in the chunk, -), blob order
+  const long long *entry_off;  // byte offset of each of those blocks in blob
   int n_chunks;
   int max_chunk_bytes;
+  int n_entries;               // writing entries with a non-empty cloud
+  int pad_;
 };
 
 struct AbcChunk {

@@ -673,14 +673,106 @@ __global__ void __launch_bounds__(256) k_abc_bulk(Abc ab, StepPtrs p, int do_the
   }
 }
 
+__device__ __forceinline__ void prefetch_l2(const void *src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(reinterpret_cast<uint64_t>(src)), "r"(bytes)
+               : "memory");
+}
+
+// The same step of the absorbing boundary, persistent: warp w of W walks the
+// writing ABC entries w, w + W, ... in blob order.  Before it works on one
+// entry, lane 0 asks the copy engine to bring the operator block of the entry
+// kLookahead visits ahead into L2 (cp.async.bulk.prefetch.L2), so the HBM
+// stream of operators runs ahead of the warps and their own loads hit L2.
+constexpr int kLookahead = 3;
+
+__global__ void __launch_bounds__(256) k_abc_l2(Abc ab, StepPtrs p, int do_theta) {
+  const int lane = threadIdx.x & 31;
+  const int W = gridDim.x * kAbcWarpsPerBlock;
+  const int w0 = blockIdx.x * kAbcWarpsPerBlock + (threadIdx.x >> 5);
+  const int n_ent = ab.n_entries;
+  if (lane == 0)
+    for (int d = 0; d < kLookahead; d++) {
+      const int f = w0 + d * W;
+      if (f < n_ent) {
+        const int4 e = ab.chunk_entries[f];
+        prefetch_l2(ab.blob + ab.entry_off[f], 152 * e.y);
+      }
+    }
+  for (int i = w0; i < n_ent; i += W) {
+    if (lane == 0) {
+      const int f = i + kLookahead * W;
+      if (f < n_ent) prefetch_l2(ab.blob + ab.entry_off[f], 152 * ab.chunk_entries[f].y);
+    }
+    const int4 ent = ab.chunk_entries[i];
+    const int a = ent.x, len = ent.y, hp = len >> 1;
+    const unsigned char *blk = ab.blob + ab.entry_off[i];
+    const double2 *__restrict__ gu = reinterpret_cast<const double2 *>(blk);
+    const double2 *__restrict__ gv = gu + 4 * len;
+    const double2 *__restrict__ gt = gv + 4 * len;
+    const int2 *__restrict__ idx = reinterpret_cast<const int2 *>(blk + 144 * len);
+    const int2 *__restrict__ src = idx + hp;
+    const InstParams &P = c_inst[ab.inst[a]];
+    const bool kin = P.kinematic != 0;
+    double ux = 0.0, uy = 0.0, vx = 0.0, vy = 0.0, th = 0.0;
+    for (int q = lane; q < hp; q += 32) {
+      const int2 k = __ldg(idx + q), s = __ldg(src + q);
+      const double2 un0 = s.x >= 0 ? p.s_prev[s.x] : p.u_n[k.x], um0 = p.u_nm1[k.x];
+      const double2 un1 = s.y >= 0 ? p.s_prev[s.y] : p.u_n[k.y], um1 = p.u_nm1[k.y];
+      const double xs[4][2] = {{un0.x, un1.x}, {un0.y, un1.y}, {um0.x, um1.x}, {um0.y, um1.y}};
+#pragma unroll
+      for (int r = 0; r < 4; r++) {
+        const double2 gx = __ldg(gu + r * hp + q), gy = __ldg(gu + (4 + r) * hp + q);
+        ux += gx.x * xs[r][0] + gx.y * xs[r][1];
+        uy += gy.x * xs[r][0] + gy.y * xs[r][1];
+      }
+      if (!kin) {
+        const double2 vn0 = p.v_n[k.x], vm0 = p.v_nm1[k.x], vn1 = p.v_n[k.y], vm1 = p.v_nm1[k.y];
+        const double ys[4][2] = {{vn0.x, vn1.x}, {vn0.y, vn1.y}, {vm0.x, vm1.x}, {vm0.y, vm1.y}};
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+          const double2 hx = __ldg(gv + r * hp + q), hy = __ldg(gv + (4 + r) * hp + q);
+          vx += hx.x * ys[r][0] + hx.y * ys[r][1];
+          vy += hy.x * ys[r][0] + hy.y * ys[r][1];
+        }
+      }
+      if (do_theta) {
+        const double2 w0v = __ldg(gt + q), w1v = __ldg(gt + hp + q);
+        th += w0v.x * p.th_n[k.x] + w0v.y * p.th_n[k.y] + w1v.x * p.th_nm1[k.x] + w1v.y * p.th_nm1[k.y];
+      }
+    }
+    ux = warp_sum(ux);
+    uy = warp_sum(uy);
+    if (!kin) {
+      vx = warp_sum(vx);
+      vy = warp_sum(vy);
+    }
+    if (do_theta) th = warp_sum(th);
+    if (lane == 0) {
+      const int node = ab.node[a];
+      p.s_abc[a] = make_double2(ux, uy);
+      if (kin) {
+        // v = (u^{n+1} - u^n) / dt with this node's u^n, src/main.cpp:940-943
+        const double2 un = p.s_prev[a];
+        p.v_np1[node] = make_double2((ux - un.x) / P.dt, (uy - un.y) / P.dt);
+      } else {
+        p.v_np1[node] = make_double2(vx, vy);
+      }
+      if (do_theta) p.th_np1[node] = th;
+    }
+  }
+}
+
 cudaError_t dense_prepare_abc(const Abc &ab, DenseGeo &dg) {
-  int dev = 0, n_sm = 0;
+  int dev = 0, n_sm = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-  dg.abc_stage = (std::max(ab.max_chunk_bytes, 16) + 127) / 128 * 128;
-  dg.abc_smem = 2 * dg.abc_stage + 64;
-  dg.abc_grid = std::max(1, std::min(ab.n_chunks, n_sm));
-  return cudaFuncSetAttribute(k_abc_bulk, cudaFuncAttributeMaxDynamicSharedMemorySize, dg.abc_smem);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_abc_l2, 256, 0);
+  if (e != cudaSuccess) return e;
+  const int need = (ab.n_entries + kAbcWarpsPerBlock - 1) / kAbcWarpsPerBlock;
+  dg.abc_grid = std::max(1, std::min(need, std::max(per_sm, 1) * n_sm));
+  dg.abc_stage = 0;
+  dg.abc_smem = 0;
+  return cudaSuccess;
 }
 
 // G_u (src/main.cpp:883-916) and G_v (:933-974) of one step for one ABC node
@@ -993,9 +1085,9 @@ int enqueue_dense_step(const DenseGeo &dg, const LaunchGeo &lg, const StepPtrs &
       cudaEventRecord(dg.ev_fork[0], st);
       cudaStreamWaitEvent(side, dg.ev_fork[0], 0);
     }
-    k_abc_bulk<<<dg.abc_grid, 256, dg.abc_smem, side>>>(lg.abc, p, gth ? 1 : 0, dg.abc_stage, dg.d_err);
+    k_abc_l2<<<dg.abc_grid, 256, 0, side>>>(lg.abc, p, gth ? 1 : 0);
     if (fork) cudaEventRecord(dg.ev_join[0], side);
-    if (mark) (*mark)("abc_bulk");
+    if (mark) (*mark)("abc_l2");
     k++;
   }
   for (const auto &gr : dg.groups) {
