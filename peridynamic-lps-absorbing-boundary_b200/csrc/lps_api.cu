@@ -689,6 +689,12 @@ int finish_dense(lps_handle *h) {
   int s;
   if ((s = dev_alloc(h, &D.d_err, 1))) return s;
   LPS_CUDA_TRY(h, cudaMemset(D.d_err, 0, sizeof(int)));
+  // tile-scheduler counters: per group (theta next, done, force next, done)
+  int *sched = nullptr;
+  const size_t n_sched = 4 * D.groups.size();
+  if ((s = dev_alloc(h, &sched, n_sched))) return s;
+  LPS_CUDA_TRY(h, cudaMemset(sched, 0, n_sched * sizeof(int)));
+  for (size_t g = 0; g < D.groups.size(); g++) D.groups[g].sched = sched + 4 * g;
   return LPS_OK;
 }
 

@@ -58,6 +58,7 @@ struct DenseGroup {
   int n_tiles;
   int grid_theta;   // persistent grid sizes
   int grid_force;
+  int *sched;       // device tile-scheduler counters (theta: [0..1], force: [2..3])
   DenseMaps maps;
 };
 
@@ -67,7 +68,8 @@ struct DenseGeo {
   int pitch = 0;
   int total_rows = 0;
   int tile_priority = 0;                       // launch priority of the tile kernels
-  int abc_grid = 1, abc_stage = 0, abc_smem = 0;  // bulk-copy ABC kernel launch shape
+  int abc_grid = 1;                            // persistent grid of the G_u/G_v kernel
+  int abc_mode = 0;                            // schedule of the absorbing-boundary kernels
   cudaStream_t side = nullptr;                 // forked stream for the ABC kernels
   cudaEvent_t ev_fork[2] = {nullptr, nullptr}, ev_join[2] = {nullptr, nullptr};
   int *d_err = nullptr;                        // device wait-timeout flag

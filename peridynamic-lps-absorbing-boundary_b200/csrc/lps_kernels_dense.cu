@@ -223,6 +223,21 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
   return false;
 }
 
+// Dynamic tile scheduler of the persistent tile kernels: a CTA takes its next
+// tile from a counter, so a CTA that becomes resident late (its SM still runs
+// blocks of the concurrent absorbing-boundary kernel) takes fewer tiles instead
+// of stretching the launch.  sched[0] is the next tile, sched[1] counts
+// finished CTAs; the last CTA to finish rewinds both for the next launch.
+__device__ __forceinline__ int sched_next(int *sched) { return atomicAdd(sched, 1); }
+
+__device__ __forceinline__ void sched_finish(int *sched) {
+  __threadfence();
+  if (atomicAdd(sched + 1, 1) == (int)gridDim.x - 1) {
+    sched[0] = 0;
+    sched[1] = 0;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Tile compute.  A thread owns cells (r0, c) and (r0 + 1, c); for every pair
 // of opposite offsets (a, b) / (-a, -b) it reads the two staged neighbours of
@@ -335,9 +350,10 @@ template <int M>
 __global__ void __launch_bounds__(kTileThreads, 2)
     k_theta_tma(const __grid_constant__ CUtensorMap map_u, const __grid_constant__ CUtensorMap map_type, Geo g,
                 const DenseTile *__restrict__ tiles, int tile_begin, int n_tiles, StepPtrs p, int pitch,
-                int skip_abc, int *err) {
+                int skip_abc, int *sched, int *err) {
   using R = Region<M>;
   extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ int s_tile[2];
   uint64_t *bar = reinterpret_cast<uint64_t *>(smem + 2 * R::THETA_STAGE);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (*(volatile int *)err) return;  // an earlier wait timed out: do nothing
@@ -345,6 +361,7 @@ __global__ void __launch_bounds__(kTileThreads, 2)
     mbar_init(&bar[0], 1);
     mbar_init(&bar[1], 1);
     mbar_fence_init();
+    s_tile[0] = sched_next(sched);
   }
   __syncthreads();
   auto issue = [&](int stage, int tile) {
@@ -354,11 +371,15 @@ __global__ void __launch_bounds__(kTileThreads, 2)
     tma_load_2d(base, &map_u, 2 * t.col, t.row, &bar[stage]);
     tma_load_2d(base + R::T_TY, &map_type, t.col, t.row, &bar[stage]);
   };
-  int tile = blockIdx.x;
+  int tile = s_tile[0];
   if (tid == 0 && tile < n_tiles) issue(0, tile);
-  for (int it = 0; tile < n_tiles; it++, tile += gridDim.x) {
+  for (int it = 0; tile < n_tiles; it++, tile = s_tile[it & 1]) {
     const int stage = it & 1;
-    if (tid == 0 && tile + (int)gridDim.x < n_tiles) issue(stage ^ 1, tile + gridDim.x);
+    if (tid == 0) {
+      const int nx = sched_next(sched);
+      s_tile[stage ^ 1] = nx;
+      if (nx < n_tiles) issue(stage ^ 1, nx);
+    }
     const DenseTile t = tiles[tile_begin + tile];
     const InstParams &P = c_inst[t.inst];
     double2 *su = reinterpret_cast<double2 *>(smem + stage * R::THETA_STAGE);
@@ -405,6 +426,7 @@ __global__ void __launch_bounds__(kTileThreads, 2)
     fence_proxy_async_smem();
     __syncthreads();  // the stage is refilled at the start of the next-but-one iteration
   }
+  if (tid == 0) sched_finish(sched);
 }
 
 // ---------------------------------------------------------------------------
@@ -416,9 +438,10 @@ __global__ void __launch_bounds__(kTileThreads, 2)
     k_force_tma(const __grid_constant__ CUtensorMap map_u, const __grid_constant__ CUtensorMap map_th,
                 const __grid_constant__ CUtensorMap map_coef, const __grid_constant__ CUtensorMap map_type, Geo g,
                 const DenseTile *__restrict__ tiles, int tile_begin, int n_tiles, StepPtrs p, int pitch, int abc_on,
-                int bump_step, int *d_step, int *err) {
+                int bump_step, int *d_step, int *sched, int *err) {
   using R = Region<M>;
   extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ int s_tile[2];
   uint64_t *bar = reinterpret_cast<uint64_t *>(smem + 2 * R::FORCE_STAGE);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (*(volatile int *)err) return;  // an earlier wait timed out: do nothing
@@ -427,6 +450,7 @@ __global__ void __launch_bounds__(kTileThreads, 2)
     mbar_init(&bar[1], 1);
     mbar_fence_init();
     if (bump_step && blockIdx.x == 0) *d_step += 1;
+    s_tile[0] = sched_next(sched);
   }
   __syncthreads();
   auto issue = [&](int stage, int tile) {
@@ -438,11 +462,15 @@ __global__ void __launch_bounds__(kTileThreads, 2)
     tma_load_2d(base + R::F_CO, &map_coef, 2 * t.col, t.row, &bar[stage]);
     tma_load_2d(base + R::F_TY, &map_type, t.col, t.row, &bar[stage]);
   };
-  int tile = blockIdx.x;
+  int tile = s_tile[0];
   if (tid == 0 && tile < n_tiles) issue(0, tile);
-  for (int it = 0; tile < n_tiles; it++, tile += gridDim.x) {
+  for (int it = 0; tile < n_tiles; it++, tile = s_tile[it & 1]) {
     const int stage = it & 1;
-    if (tid == 0 && tile + (int)gridDim.x < n_tiles) issue(stage ^ 1, tile + gridDim.x);
+    if (tid == 0) {
+      const int nx = sched_next(sched);
+      s_tile[stage ^ 1] = nx;
+      if (nx < n_tiles) issue(stage ^ 1, nx);
+    }
     const DenseTile t = tiles[tile_begin + tile];
     const InstParams &P = c_inst[t.inst];
     unsigned char *base = smem + stage * R::FORCE_STAGE;
@@ -493,6 +521,7 @@ __global__ void __launch_bounds__(kTileThreads, 2)
     fence_proxy_async_smem();
     __syncthreads();
   }
+  if (tid == 0) sched_finish(sched);
 }
 
 // ---------------------------------------------------------------------------
@@ -507,202 +536,33 @@ __global__ void __launch_bounds__(256) k_abc_uv(Abc ab, StepPtrs p) {
   abc_uv_warp(ab, a, p);
 }
 
-// G_theta (src/main.cpp:795-812), G_u (:883-916) and G_v (:933-974) of one
-// step for one ABC node per warp, dense path.  Clouds are padded to an even
-// length, so each lane owns an entry pair and reads every operator row as one
-// aligned double2.  It runs while the dilatation tiles of the same step are
-// predicting and merging displacements: u^n of a cloud node that is itself
-// G_u-written comes from the previous step's G_u result (p.s_prev) and the
-// new result goes to the other buffer (p.s_abc).
-__global__ void __launch_bounds__(256, 3) k_abc_dense(Abc ab, StepPtrs p, int do_theta) {
-  const int lane = threadIdx.x & 31;
-  const int a = blockIdx.x * kAbcWarpsPerBlock + (threadIdx.x >> 5);
-  if (a >= ab.n_abc || !ab.writes[a]) return;
-  const InstParams &P = c_inst[ab.inst[a]];
-  const int off = ab.cl_off[a], hp = ab.cl_len[a] >> 1;  // entry pairs
-  const double2 *__restrict__ gu = reinterpret_cast<const double2 *>(ab.gu + 8 * (size_t)off);
-  const double2 *__restrict__ gv = reinterpret_cast<const double2 *>(ab.gv + 8 * (size_t)off);
-  const double2 *__restrict__ gt = reinterpret_cast<const double2 *>(ab.gth + 2 * (size_t)off);
-  const int2 *__restrict__ idx = reinterpret_cast<const int2 *>(ab.cl_idx + off);
-  const int2 *__restrict__ src = reinterpret_cast<const int2 *>(ab.cl_src + off);
-  const bool kin = P.kinematic != 0;
-  double ux = 0.0, uy = 0.0, vx = 0.0, vy = 0.0, th = 0.0;
-  for (int q = lane; q < hp; q += 32) {
-    const int2 k = __ldg(idx + q), s = __ldg(src + q);
-    const double2 un0 = s.x >= 0 ? p.s_prev[s.x] : p.u_n[k.x], um0 = p.u_nm1[k.x];
-    const double2 un1 = s.y >= 0 ? p.s_prev[s.y] : p.u_n[k.y], um1 = p.u_nm1[k.y];
-    const double xs[4][2] = {{un0.x, un1.x}, {un0.y, un1.y}, {um0.x, um1.x}, {um0.y, um1.y}};
-#pragma unroll
-    for (int r = 0; r < 4; r++) {
-      const double2 gx = __ldg(gu + r * hp + q), gy = __ldg(gu + (4 + r) * hp + q);
-      ux += gx.x * xs[r][0] + gx.y * xs[r][1];
-      uy += gy.x * xs[r][0] + gy.y * xs[r][1];
-    }
-    if (!kin) {
-      const double2 vn0 = p.v_n[k.x], vm0 = p.v_nm1[k.x], vn1 = p.v_n[k.y], vm1 = p.v_nm1[k.y];
-      const double ys[4][2] = {{vn0.x, vn1.x}, {vn0.y, vn1.y}, {vm0.x, vm1.x}, {vm0.y, vm1.y}};
-#pragma unroll
-      for (int r = 0; r < 4; r++) {
-        const double2 hx = __ldg(gv + r * hp + q), hy = __ldg(gv + (4 + r) * hp + q);
-        vx += hx.x * ys[r][0] + hx.y * ys[r][1];
-        vy += hy.x * ys[r][0] + hy.y * ys[r][1];
-      }
-    }
-    if (do_theta) {
-      const double2 w0 = __ldg(gt + q), w1 = __ldg(gt + hp + q);
-      th += w0.x * p.th_n[k.x] + w0.y * p.th_n[k.y] + w1.x * p.th_nm1[k.x] + w1.y * p.th_nm1[k.y];
-    }
-  }
-  ux = warp_sum(ux);
-  uy = warp_sum(uy);
-  if (!kin) {
-    vx = warp_sum(vx);
-    vy = warp_sum(vy);
-  }
-  if (do_theta) th = warp_sum(th);
-  if (lane == 0) {
-    const int node = ab.node[a];
-    p.s_abc[a] = make_double2(ux, uy);
-    if (kin) {
-      // v = (u^{n+1} - u^n) / dt with this node's u^n, src/main.cpp:940-943
-      const double2 un = p.s_prev[a];
-      p.v_np1[node] = make_double2((ux - un.x) / P.dt, (uy - un.y) / P.dt);
-    } else {
-      p.v_np1[node] = make_double2(vx, vy);
-    }
-    if (do_theta) p.th_np1[node] = th;
-  }
-}
-
-__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                   smem_u32(dst)),
-               "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(smem_u32(bar))
-               : "memory");
-}
-
-// The same step of the absorbing boundary as k_abc_dense, persistent over
-// chunks of operator blocks that bulk copies (cp.async.bulk) stream into two
-// shared-memory stages: while the warps of a CTA apply the operators of one
-// chunk (an ABC node per warp, entry pairs per lane, history gathered from
-// global memory), the next chunk is already in flight.  One CTA per SM.
-__global__ void __launch_bounds__(256) k_abc_bulk(Abc ab, StepPtrs p, int do_theta, int stage_bytes, int *err) {
-  extern __shared__ __align__(128) unsigned char smem[];
-  uint64_t *bar = reinterpret_cast<uint64_t *>(smem + 2 * stage_bytes);
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  if (*(volatile int *)err) return;
-  if (tid == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
-    mbar_fence_init();
-  }
-  __syncthreads();
-  auto issue = [&](int stage, int c) {
-    const AbcChunk ch = ab.chunks[c];
-    mbar_expect_tx(&bar[stage], ch.bytes);
-    bulk_load(smem + stage * stage_bytes, ab.blob + ch.off, ch.bytes, &bar[stage]);
-  };
-  int c = blockIdx.x;
-  if (tid == 0 && c < ab.n_chunks) issue(0, c);
-  for (int it = 0; c < ab.n_chunks; it++, c += gridDim.x) {
-    const int stage = it & 1;
-    if (tid == 0 && c + (int)gridDim.x < ab.n_chunks) issue(stage ^ 1, c + gridDim.x);
-    const AbcChunk ch = ab.chunks[c];
-    int4 ent = make_int4(0, 0, 0, 0);
-    if (warp < ch.count) ent = ab.chunk_entries[ch.first + warp];
-    if (!mbar_wait_bounded(&bar[stage], (it >> 1) & 1, err)) return;
-    if (warp < ch.count) {
-      const int a = ent.x, len = ent.y, hp = len >> 1;
-      const unsigned char *blk = smem + stage * stage_bytes + ent.z;
-      const double2 *gu = reinterpret_cast<const double2 *>(blk);
-      const double2 *gv = gu + 4 * len;
-      const double2 *gt = gv + 4 * len;
-      const int2 *idx = reinterpret_cast<const int2 *>(blk + 144 * len);
-      const int2 *src = idx + hp;
-      const InstParams &P = c_inst[ab.inst[a]];
-      const bool kin = P.kinematic != 0;
-      double ux = 0.0, uy = 0.0, vx = 0.0, vy = 0.0, th = 0.0;
-      for (int q = lane; q < hp; q += 32) {
-        const int2 k = idx[q], s = src[q];
-        const double2 un0 = s.x >= 0 ? p.s_prev[s.x] : p.u_n[k.x], um0 = p.u_nm1[k.x];
-        const double2 un1 = s.y >= 0 ? p.s_prev[s.y] : p.u_n[k.y], um1 = p.u_nm1[k.y];
-        const double xs[4][2] = {{un0.x, un1.x}, {un0.y, un1.y}, {um0.x, um1.x}, {um0.y, um1.y}};
-#pragma unroll
-        for (int r = 0; r < 4; r++) {
-          const double2 gx = gu[r * hp + q], gy = gu[(4 + r) * hp + q];
-          ux += gx.x * xs[r][0] + gx.y * xs[r][1];
-          uy += gy.x * xs[r][0] + gy.y * xs[r][1];
-        }
-        if (!kin) {
-          const double2 vn0 = p.v_n[k.x], vm0 = p.v_nm1[k.x], vn1 = p.v_n[k.y], vm1 = p.v_nm1[k.y];
-          const double ys[4][2] = {{vn0.x, vn1.x}, {vn0.y, vn1.y}, {vm0.x, vm1.x}, {vm0.y, vm1.y}};
-#pragma unroll
-          for (int r = 0; r < 4; r++) {
-            const double2 hx = gv[r * hp + q], hy = gv[(4 + r) * hp + q];
-            vx += hx.x * ys[r][0] + hx.y * ys[r][1];
-            vy += hy.x * ys[r][0] + hy.y * ys[r][1];
-          }
-        }
-        if (do_theta) {
-          const double2 w0 = gt[q], w1 = gt[hp + q];
-          th += w0.x * p.th_n[k.x] + w0.y * p.th_n[k.y] + w1.x * p.th_nm1[k.x] + w1.y * p.th_nm1[k.y];
-        }
-      }
-      ux = warp_sum(ux);
-      uy = warp_sum(uy);
-      if (!kin) {
-        vx = warp_sum(vx);
-        vy = warp_sum(vy);
-      }
-      if (do_theta) th = warp_sum(th);
-      if (lane == 0) {
-        const int node = ab.node[a];
-        p.s_abc[a] = make_double2(ux, uy);
-        if (kin) {
-          // v = (u^{n+1} - u^n) / dt with this node's u^n, src/main.cpp:940-943
-          const double2 un = p.s_prev[a];
-          p.v_np1[node] = make_double2((ux - un.x) / P.dt, (uy - un.y) / P.dt);
-        } else {
-          p.v_np1[node] = make_double2(vx, vy);
-        }
-        if (do_theta) p.th_np1[node] = th;
-      }
-    }
-    fence_proxy_async_smem();
-    __syncthreads();  // the stage is refilled at the start of the next-but-one iteration
-  }
-}
-
 __device__ __forceinline__ void prefetch_l2(const void *src, uint32_t bytes) {
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(reinterpret_cast<uint64_t>(src)), "r"(bytes)
                : "memory");
 }
 
-// The same step of the absorbing boundary, persistent: warp w of W walks the
-// writing ABC entries w, w + W, ... in blob order.  Before it works on one
-// entry, lane 0 asks the copy engine to bring the operator block of the entry
-// kLookahead visits ahead into L2 (cp.async.bulk.prefetch.L2), so the HBM
-// stream of operators runs ahead of the warps and their own loads hit L2.
-constexpr int kLookahead = 3;
-
-__global__ void __launch_bounds__(256) k_abc_l2(Abc ab, StepPtrs p, int do_theta) {
+// G_u (src/main.cpp:883-916), G_v (:933-974) and optionally G_theta
+// (:795-812) of one step, one writing ABC entry per warp, dense path.  The
+// operators come from the entry's contiguous block in Abc::blob (clouds padded
+// to an even length, so a lane owns an entry pair and reads each operator row
+// as one aligned double2).  Warp w of W takes entries w, w + W, ...; before
+// entry i, lane 0 has the copy engine bring the block of entry i + pf into L2
+// (cp.async.bulk.prefetch.L2), so the HBM stream of operators runs ahead of
+// the warps' own loads.  The kernel runs while the tile kernels of the same
+// step merge and predict displacements: u^n of a cloud node that is itself
+// G_u-written comes from the previous step's G_u result (p.s_prev), and the
+// result goes to the other buffer (p.s_abc).  At most 80 registers, so one
+// block fits beside two dilatation CTAs on an SM.
+__global__ void __launch_bounds__(256, 3) k_abc_l2(Abc ab, StepPtrs p, int do_theta, int pf) {
   const int lane = threadIdx.x & 31;
   const int W = gridDim.x * kAbcWarpsPerBlock;
   const int w0 = blockIdx.x * kAbcWarpsPerBlock + (threadIdx.x >> 5);
   const int n_ent = ab.n_entries;
-  if (lane == 0)
-    for (int d = 0; d < kLookahead; d++) {
-      const int f = w0 + d * W;
-      if (f < n_ent) {
-        const int4 e = ab.chunk_entries[f];
-        prefetch_l2(ab.blob + ab.entry_off[f], 152 * e.y);
-      }
-    }
+  if (lane == 0 && pf >= W)
+    for (int f = w0 + W; f < w0 + pf && f < n_ent; f += W)
+      prefetch_l2(ab.blob + ab.entry_off[f], 152 * ab.chunk_entries[f].y);
   for (int i = w0; i < n_ent; i += W) {
-    if (lane == 0) {
-      const int f = i + kLookahead * W;
-      if (f < n_ent) prefetch_l2(ab.blob + ab.entry_off[f], 152 * ab.chunk_entries[f].y);
-    }
+    if (lane == 0 && i + pf < n_ent) prefetch_l2(ab.blob + ab.entry_off[i + pf], 152 * ab.chunk_entries[i + pf].y);
     const int4 ent = ab.chunk_entries[i];
     const int a = ent.x, len = ent.y, hp = len >> 1;
     const unsigned char *blk = ab.blob + ab.entry_off[i];
@@ -769,9 +629,10 @@ cudaError_t dense_prepare_abc(const Abc &ab, DenseGeo &dg) {
   cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_abc_l2, 256, 0);
   if (e != cudaSuccess) return e;
   const int need = (ab.n_entries + kAbcWarpsPerBlock - 1) / kAbcWarpsPerBlock;
-  dg.abc_grid = std::max(1, std::min(need, std::max(per_sm, 1) * n_sm));
-  dg.abc_stage = 0;
-  dg.abc_smem = 0;
+  const char *mode = getenv("LPS_DENSE_ABC_MODE");
+  dg.abc_mode = mode ? atoi(mode) : 0;
+  const int per = dg.abc_mode == 3 ? 1 : std::max(per_sm, 1);
+  dg.abc_grid = std::max(1, std::min(need, per * n_sm));
   return cudaSuccess;
 }
 
@@ -1056,7 +917,7 @@ static void launch_theta_group(const DenseGroup &gr, const LaunchGeo &lg, const 
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   cudaLaunchKernelEx(&cfg, k_theta_tma<M>, gr.maps.u[ring_u], gr.maps.type, lg.geo, dg.tiles, gr.tile_begin,
-                     gr.n_tiles, p, dg.pitch, skip_abc ? 1 : 0, dg.d_err);
+                     gr.n_tiles, p, dg.pitch, skip_abc ? 1 : 0, gr.sched, dg.d_err);
 }
 
 template <int M>
@@ -1064,7 +925,7 @@ static void launch_force_group(const DenseGroup &gr, const LaunchGeo &lg, const 
                                int ring_u, int ring_th, bool abc_on, bool first, int *d_step, cudaStream_t st) {
   k_force_tma<M><<<gr.grid_force, kTileThreads, Region<M>::FORCE_SMEM, st>>>(
       gr.maps.u[ring_u], gr.maps.th[ring_th], gr.maps.coef, gr.maps.type, lg.geo, dg.tiles, gr.tile_begin,
-      gr.n_tiles, p, dg.pitch, abc_on ? 1 : 0, first ? 1 : 0, d_step, dg.d_err);
+      gr.n_tiles, p, dg.pitch, abc_on ? 1 : 0, first ? 1 : 0, d_step, gr.sched + 2, dg.d_err);
 }
 
 // ring_u: index of u^{n+1} (the predicted level) in the 4-deep ring;
@@ -1080,15 +941,43 @@ int enqueue_dense_step(const DenseGeo &dg, const LaunchGeo &lg, const StepPtrs &
   const bool fork = mark == nullptr;
   cudaStream_t side = fork ? dg.side : st;
   // pass 1: G_theta, G_u, G_v of this step || predicted u -> theta tiles
+  const int mode = dg.abc_mode;
+  const int W = dg.abc_grid * kAbcWarpsPerBlock;
+  const int n_blk = (lg.abc.n_abc + kAbcWarpsPerBlock - 1) / kAbcWarpsPerBlock;
+  const int n_ent_blk = (lg.abc.n_entries + kAbcWarpsPerBlock - 1) / kAbcWarpsPerBlock;
+  bool late_join = false;  // the G_u/G_v kernel may run on through the force tiles
   if (abc) {
     if (fork) {
       cudaEventRecord(dg.ev_fork[0], st);
       cudaStreamWaitEvent(side, dg.ev_fork[0], 0);
     }
-    k_abc_l2<<<dg.abc_grid, 256, 0, side>>>(lg.abc, p, gth ? 1 : 0);
-    if (fork) cudaEventRecord(dg.ev_join[0], side);
-    if (mark) (*mark)("abc_l2");
-    k++;
+    if (mode == 0) {
+      k_abc_l2<<<dg.abc_grid, 256, 0, side>>>(lg.abc, p, gth ? 1 : 0, 3 * W);
+      if (fork) cudaEventRecord(dg.ev_join[0], side);
+      if (mark) (*mark)("abc_l2");
+      k++;
+    } else {
+      if (gth) {
+        k_abc_theta<<<n_blk, 256, 0, side>>>(lg.abc, p.th_n, p.th_nm1, p.th_np1);
+        if (mark) (*mark)("abc_theta");
+        k++;
+      }
+      if (mode == 1 || mode == 4) {
+        if (mode == 4 && fork) cudaEventRecord(dg.ev_join[0], side);
+        k_abc_uv_dense<<<n_blk, 256, 0, side>>>(lg.abc, p);
+        if (mark) (*mark)("abc_uv");
+      } else {
+        if (fork) cudaEventRecord(dg.ev_join[0], side);
+        if (mode == 2)
+          k_abc_l2<<<n_ent_blk, 256, 0, side>>>(lg.abc, p, 0, 4096);
+        else
+          k_abc_l2<<<dg.abc_grid, 256, 0, side>>>(lg.abc, p, 0, 3 * W);
+        if (mark) (*mark)("abc_uv");
+      }
+      k++;
+      late_join = mode != 1;
+      if (fork) cudaEventRecord(dg.ev_join[late_join ? 1 : 0], side);
+    }
   }
   for (const auto &gr : dg.groups) {
     LPS_DISPATCH_M(gr.m, launch_theta_group, gr, lg, dg, p, ring_u, gth, st);
@@ -1108,6 +997,7 @@ int enqueue_dense_step(const DenseGeo &dg, const LaunchGeo &lg, const StepPtrs &
     first = false;
     k++;
   }
+  if (abc && fork && late_join) cudaStreamWaitEvent(st, dg.ev_join[1], 0);
   if (mark) (*mark)("force_tiles");
   return k;
 }
