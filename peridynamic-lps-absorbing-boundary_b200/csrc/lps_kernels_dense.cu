@@ -353,8 +353,10 @@ __global__ void __launch_bounds__(kTileThreads, 2)
                 int skip_abc, int *sched, int *err) {
   using R = Region<M>;
   extern __shared__ __align__(128) unsigned char smem[];
-  __shared__ int s_tile[2];
   uint64_t *bar = reinterpret_cast<uint64_t *>(smem + 2 * R::THETA_STAGE);
+  // next tiles of the two stages, beside the barriers: static shared memory
+  // would shift the dynamic buffer off its 128-byte alignment
+  int *s_tile = reinterpret_cast<int *>(bar + 2);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (*(volatile int *)err) return;  // an earlier wait timed out: do nothing
   if (tid == 0) {
@@ -441,8 +443,10 @@ __global__ void __launch_bounds__(kTileThreads, 2)
                 int bump_step, int *d_step, int *sched, int *err) {
   using R = Region<M>;
   extern __shared__ __align__(128) unsigned char smem[];
-  __shared__ int s_tile[2];
   uint64_t *bar = reinterpret_cast<uint64_t *>(smem + 2 * R::FORCE_STAGE);
+  // next tiles of the two stages, beside the barriers: static shared memory
+  // would shift the dynamic buffer off its 128-byte alignment
+  int *s_tile = reinterpret_cast<int *>(bar + 2);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (*(volatile int *)err) return;  // an earlier wait timed out: do nothing
   if (tid == 0) {
