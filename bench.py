@@ -204,8 +204,6 @@ def algorithmic_bytes(sets, kernel):
         "abc_uv": (132 * abc, None),
         # G_theta: 2C doubles + 4C index bytes per ABC node
         "abc_theta": (20 * abc, None),
-        # G_u, G_v and G_theta in one pass: 18C doubles + 4C index bytes
-        "abc_l2": (148 * abc, None),
         # neighbour-list path
         "predict_csr": (80 * n, None),
         "theta_csr": (32 * n, None),

@@ -266,68 +266,6 @@ int upload_abc(lps_handle *h, const HostAbc &H, int total_abc, const std::vector
   return LPS_OK;
 }
 
-// Dense path: the operators of every writing ABC entry again as one
-// contiguous block (see Abc::blob), grouped into chunks of at most 8 entries
-// and kAbcChunkBytes bytes (a single entry may exceed that and gets a chunk
-// of its own).  Each chunk is one bulk copy into shared memory.
-constexpr int kAbcChunkBytes = 64 * 1024;
-
-int upload_abc_blob(lps_handle *h, const HostAbc &H, const std::vector<int> &abc_of) {
-  Abc &B = h->lg.abc;
-  std::vector<unsigned char> blob;
-  std::vector<AbcChunk> chunks;
-  std::vector<int4> ents;
-  std::vector<long long> ent_off;
-  AbcChunk cur{0, 0, 0, 0, 0};
-  int max_bytes = 0;
-  auto push_bytes = [&blob](const void *src, size_t n) {
-    const unsigned char *s = static_cast<const unsigned char *>(src);
-    blob.insert(blob.end(), s, s + n);
-  };
-  for (size_t a = 0; a < H.writes.size(); a++) {
-    const int len = H.cl_len[a];
-    if (!H.writes[a] || len == 0) continue;
-    const int bytes = 152 * len;  // 18 rows of doubles + 2 rows of ints; len is even
-    if (cur.count > 0 && (cur.count == kAbcWarpsPerBlock || cur.bytes + bytes > kAbcChunkBytes)) {
-      chunks.push_back(cur);
-      max_bytes = std::max(max_bytes, cur.bytes);
-      cur = AbcChunk{(long long)blob.size(), (int)ents.size(), 0, 0, 0};
-    }
-    const size_t off = H.cl_off[a];
-    ent_off.push_back((long long)blob.size());
-    push_bytes(&H.gu[8 * off], sizeof(double) * 8 * len);
-    push_bytes(&H.gv[8 * off], sizeof(double) * 8 * len);
-    push_bytes(&H.gth[2 * off], sizeof(double) * 2 * len);
-    push_bytes(&H.cl_idx[off], sizeof(int) * len);
-    std::vector<int> src(len);
-    for (int e = 0; e < len; e++) src[e] = abc_of[H.cl_idx[off + e]];
-    push_bytes(src.data(), sizeof(int) * len);
-    ents.push_back(make_int4((int)a, len, cur.bytes, 0));
-    cur.count++;
-    cur.bytes += bytes;
-  }
-  if (cur.count > 0) {
-    chunks.push_back(cur);
-    max_bytes = std::max(max_bytes, cur.bytes);
-  }
-  unsigned char *d_blob;
-  AbcChunk *d_chunks;
-  int4 *d_ents;
-  long long *d_ent_off;
-  int s;
-  if ((s = dev_upload(h, &d_blob, blob)) || (s = dev_upload(h, &d_chunks, chunks)) ||
-      (s = dev_upload(h, &d_ents, ents)) || (s = dev_upload(h, &d_ent_off, ent_off)))
-    return s;
-  B.blob = d_blob;
-  B.chunks = d_chunks;
-  B.chunk_entries = d_ents;
-  B.entry_off = d_ent_off;
-  B.n_chunks = (int)chunks.size();
-  B.max_chunk_bytes = max_bytes;
-  B.n_entries = (int)ents.size();
-  return LPS_OK;
-}
-
 // ---------------------------------------------------------------------------
 int build_csr(lps_handle *h, const lps_problem *probs) {
   const int K = h->n_inst;
@@ -393,7 +331,6 @@ int build_csr(lps_handle *h, const lps_problem *probs) {
   }
   // upload
   Geo &G = h->lg.geo;
-  Abc &B = h->lg.abc;
   G.n_total = total;
   G.ell_width = width;
   double2 *d_xy, *d_coef;
@@ -654,7 +591,6 @@ int build_dense(lps_handle *h, const lps_problem *probs, const std::vector<Latti
   G.len = nullptr; G.nbr = nullptr;
   D.tiles = d_tiles;
   if ((st = upload_abc(h, H, total_abc, abc_of))) return st;
-  if ((st = upload_abc_blob(h, H, abc_of))) return st;
   std::map<int, int> done;
   for (int k = 0; k < K; k++) {
     if (done.count(lat[k].M)) continue;
@@ -662,7 +598,6 @@ int build_dense(lps_handle *h, const lps_problem *probs, const std::vector<Latti
     LPS_CUDA_TRY(h, upload_dense_constants(lat[k].M, probs[k].dx, probs[k].dy, probs[k].delta, h->stream));
   }
   LPS_CUDA_TRY(h, dense_prepare(D));
-  LPS_CUDA_TRY(h, dense_prepare_abc(h->lg.abc, D));
   h->lg.n_node_blocks = n / kNodeBlock;
   h->lg.n_abc_blocks = total_abc / kAbcWarpsPerBlock;
   h->lg.n_inst = K;

@@ -68,8 +68,6 @@ struct DenseGeo {
   int pitch = 0;
   int total_rows = 0;
   int tile_priority = 0;                       // launch priority of the tile kernels
-  int abc_grid = 1;                            // persistent grid of the G_u/G_v kernel
-  int abc_mode = 0;                            // schedule of the absorbing-boundary kernels
   cudaStream_t side = nullptr;                 // forked stream for the ABC kernels
   cudaEvent_t ev_fork[2] = {nullptr, nullptr}, ev_join[2] = {nullptr, nullptr};
   int *d_err = nullptr;                        // device wait-timeout flag
@@ -95,10 +93,9 @@ int dense_encode_maps(DenseGroup &g, int pitch, int total_rows, double2 *const *
                       const double2 *coef, const uint8_t *type, std::string &err);
 // Sets shared-memory limits and the persistent grid sizes of each group.
 cudaError_t dense_prepare(DenseGeo &dg);
-// Launch shape of the bulk-copy absorbing-boundary kernel.
-cudaError_t dense_prepare_abc(const Abc &ab, DenseGeo &dg);
 
-// One time step: theta tiles || G_theta, [IDW], force tiles || G_u/G_v.
+// One time step: theta tiles || G_theta, [IDW], force tiles; G_u/G_v runs
+// beside both tile passes.
 int enqueue_dense_step(const DenseGeo &dg, const LaunchGeo &lg, const StepPtrs &p, int *d_step,
                        cudaStream_t st, const Mark *mark, int ring_u);
 // Reset helpers: predicted u^1 and vh for every cell from u^0, v^0.

@@ -103,26 +103,6 @@ struct Abc {
   const int *idw_off, *idw_len;// IDW neighbour lists (THETA_ABC_METHOD 0)
   const int *idw_idx;
   const double *idw_w;
-  // Dense path: the same operators again as one contiguous block per writing
-  // entry -- [G_u 8 rows][G_v 8 rows][G_theta 2 rows] of len doubles, then
-  // cl_idx and cl_src (len ints each) -- grouped into chunks of consecutive
-  // blocks that one bulk copy brings into shared memory.
-  const unsigned char *blob;
-  const struct AbcChunk *chunks;
-  const int4 *chunk_entries;   // (ABC entry, len, byte offset in the chunk, -), blob order
-  const long long *entry_off;  // byte offset of each of those blocks in blob
-  int n_chunks;
-  int max_chunk_bytes;
-  int n_entries;               // writing entries with a non-empty cloud
-  int pad_;
-};
-
-struct AbcChunk {
-  long long off;               // byte offset of the chunk in blob
-  int first;                   // first of its entries in chunk_entries
-  int count;                   // entries (at most one per warp)
-  int bytes;                   // multiple of 16
-  int pad;
 };
 
 // Per-block partial sums of the diagnostics (src/main.cpp:986-1062).

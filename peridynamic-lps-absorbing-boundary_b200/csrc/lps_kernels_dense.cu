@@ -1,19 +1,18 @@
 // lps_kernels_dense.cu -- masked dense-grid stencil kernels, FP64, sm_100a.
 //
-// One time step is two persistent tile kernels, each with a concurrent
-// absorbing-boundary kernel on a forked stream:
-//   k_theta_tma<M>  || k_abc_theta   dilatation (src/main.cpp:736-761) of the
-//                                    predicted displacements || G_theta (:792-812)
-//   k_force_tma<M>  || k_abc_uv      force (:821-874), corrector (:922-925) and
-//                                    the next step's predictor (:725-728)
-//                                    || G_u, G_v (:883-916, :933-974)
+// One time step is two persistent tile kernels on the main stream and the
+// absorbing-boundary kernels on a forked stream:
+//   k_theta_tma<M>   dilatation (src/main.cpp:736-761) of the predicted
+//                    displacements      || k_abc_theta: G_theta (:792-812)
+//   k_force_tma<M>   force (:821-874), corrector (:922-925) and the next
+//                    step's predictor (:725-728)
+//   k_abc_uv_dense   G_u, G_v (:883-916, :933-974), beside both tile passes
 // Tile kernels stage a 16 x 32 tile plus its m-cell halo with TMA
 // (cp.async.bulk.tensor) into one of two shared-memory buffers while the
 // other buffer is being computed; every wait on the transaction barrier is
-// bounded and reports a timeout through an error flag.  Each thread owns 4
-// consecutive rows of one column and walks the stencil column by column,
-// pairing offset (a, b) with (-a, -b), so every staged value it loads feeds
-// several bonds.
+// bounded and reports a timeout through an error flag.  Each thread owns 2
+// adjacent rows of one column and walks the stencil, pairing offset (a, b)
+// with (-a, -b), so every staged value it loads feeds several bonds.
 #include <cmath>
 #include <cstdio>
 
@@ -540,106 +539,6 @@ __global__ void __launch_bounds__(256) k_abc_uv(Abc ab, StepPtrs p) {
   abc_uv_warp(ab, a, p);
 }
 
-__device__ __forceinline__ void prefetch_l2(const void *src, uint32_t bytes) {
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(reinterpret_cast<uint64_t>(src)), "r"(bytes)
-               : "memory");
-}
-
-// G_u (src/main.cpp:883-916), G_v (:933-974) and optionally G_theta
-// (:795-812) of one step, one writing ABC entry per warp, dense path.  The
-// operators come from the entry's contiguous block in Abc::blob (clouds padded
-// to an even length, so a lane owns an entry pair and reads each operator row
-// as one aligned double2).  Warp w of W takes entries w, w + W, ...; before
-// entry i, lane 0 has the copy engine bring the block of entry i + pf into L2
-// (cp.async.bulk.prefetch.L2), so the HBM stream of operators runs ahead of
-// the warps' own loads.  The kernel runs while the tile kernels of the same
-// step merge and predict displacements: u^n of a cloud node that is itself
-// G_u-written comes from the previous step's G_u result (p.s_prev), and the
-// result goes to the other buffer (p.s_abc).  At most 80 registers, so one
-// block fits beside two dilatation CTAs on an SM.
-__global__ void __launch_bounds__(256, 3) k_abc_l2(Abc ab, StepPtrs p, int do_theta, int pf) {
-  const int lane = threadIdx.x & 31;
-  const int W = gridDim.x * kAbcWarpsPerBlock;
-  const int w0 = blockIdx.x * kAbcWarpsPerBlock + (threadIdx.x >> 5);
-  const int n_ent = ab.n_entries;
-  if (lane == 0 && pf >= W)
-    for (int f = w0 + W; f < w0 + pf && f < n_ent; f += W)
-      prefetch_l2(ab.blob + ab.entry_off[f], 152 * ab.chunk_entries[f].y);
-  for (int i = w0; i < n_ent; i += W) {
-    if (lane == 0 && i + pf < n_ent) prefetch_l2(ab.blob + ab.entry_off[i + pf], 152 * ab.chunk_entries[i + pf].y);
-    const int4 ent = ab.chunk_entries[i];
-    const int a = ent.x, len = ent.y, hp = len >> 1;
-    const unsigned char *blk = ab.blob + ab.entry_off[i];
-    const double2 *__restrict__ gu = reinterpret_cast<const double2 *>(blk);
-    const double2 *__restrict__ gv = gu + 4 * len;
-    const double2 *__restrict__ gt = gv + 4 * len;
-    const int2 *__restrict__ idx = reinterpret_cast<const int2 *>(blk + 144 * len);
-    const int2 *__restrict__ src = idx + hp;
-    const InstParams &P = c_inst[ab.inst[a]];
-    const bool kin = P.kinematic != 0;
-    double ux = 0.0, uy = 0.0, vx = 0.0, vy = 0.0, th = 0.0;
-    for (int q = lane; q < hp; q += 32) {
-      const int2 k = __ldg(idx + q), s = __ldg(src + q);
-      const double2 un0 = s.x >= 0 ? p.s_prev[s.x] : p.u_n[k.x], um0 = p.u_nm1[k.x];
-      const double2 un1 = s.y >= 0 ? p.s_prev[s.y] : p.u_n[k.y], um1 = p.u_nm1[k.y];
-      const double xs[4][2] = {{un0.x, un1.x}, {un0.y, un1.y}, {um0.x, um1.x}, {um0.y, um1.y}};
-#pragma unroll
-      for (int r = 0; r < 4; r++) {
-        const double2 gx = __ldg(gu + r * hp + q), gy = __ldg(gu + (4 + r) * hp + q);
-        ux += gx.x * xs[r][0] + gx.y * xs[r][1];
-        uy += gy.x * xs[r][0] + gy.y * xs[r][1];
-      }
-      if (!kin) {
-        const double2 vn0 = p.v_n[k.x], vm0 = p.v_nm1[k.x], vn1 = p.v_n[k.y], vm1 = p.v_nm1[k.y];
-        const double ys[4][2] = {{vn0.x, vn1.x}, {vn0.y, vn1.y}, {vm0.x, vm1.x}, {vm0.y, vm1.y}};
-#pragma unroll
-        for (int r = 0; r < 4; r++) {
-          const double2 hx = __ldg(gv + r * hp + q), hy = __ldg(gv + (4 + r) * hp + q);
-          vx += hx.x * ys[r][0] + hx.y * ys[r][1];
-          vy += hy.x * ys[r][0] + hy.y * ys[r][1];
-        }
-      }
-      if (do_theta) {
-        const double2 w0v = __ldg(gt + q), w1v = __ldg(gt + hp + q);
-        th += w0v.x * p.th_n[k.x] + w0v.y * p.th_n[k.y] + w1v.x * p.th_nm1[k.x] + w1v.y * p.th_nm1[k.y];
-      }
-    }
-    ux = warp_sum(ux);
-    uy = warp_sum(uy);
-    if (!kin) {
-      vx = warp_sum(vx);
-      vy = warp_sum(vy);
-    }
-    if (do_theta) th = warp_sum(th);
-    if (lane == 0) {
-      const int node = ab.node[a];
-      p.s_abc[a] = make_double2(ux, uy);
-      if (kin) {
-        // v = (u^{n+1} - u^n) / dt with this node's u^n, src/main.cpp:940-943
-        const double2 un = p.s_prev[a];
-        p.v_np1[node] = make_double2((ux - un.x) / P.dt, (uy - un.y) / P.dt);
-      } else {
-        p.v_np1[node] = make_double2(vx, vy);
-      }
-      if (do_theta) p.th_np1[node] = th;
-    }
-  }
-}
-
-cudaError_t dense_prepare_abc(const Abc &ab, DenseGeo &dg) {
-  int dev = 0, n_sm = 0, per_sm = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_abc_l2, 256, 0);
-  if (e != cudaSuccess) return e;
-  const int need = (ab.n_entries + kAbcWarpsPerBlock - 1) / kAbcWarpsPerBlock;
-  const char *mode = getenv("LPS_DENSE_ABC_MODE");
-  dg.abc_mode = mode ? atoi(mode) : 0;
-  const int per = dg.abc_mode == 3 ? 1 : std::max(per_sm, 1);
-  dg.abc_grid = std::max(1, std::min(need, per * n_sm));
-  return cudaSuccess;
-}
-
 // G_u (src/main.cpp:883-916) and G_v (:933-974) of one step for one ABC node
 // per warp, for the dense path.  It runs while the dilatation tiles of the
 // same step are predicting and merging displacements, so u^n of a cloud node
@@ -944,44 +843,26 @@ int enqueue_dense_step(const DenseGeo &dg, const LaunchGeo &lg, const StepPtrs &
   // (serialised), so each kernel's device time can be read between events.
   const bool fork = mark == nullptr;
   cudaStream_t side = fork ? dg.side : st;
-  // pass 1: G_theta, G_u, G_v of this step || predicted u -> theta tiles
-  const int mode = dg.abc_mode;
-  const int W = dg.abc_grid * kAbcWarpsPerBlock;
+  // pass 1: G_theta || predicted u -> theta tiles.  G_u/G_v follows G_theta
+  // on the side stream and runs on beside the force tiles: its results (the
+  // G_u buffer, v at ABC nodes) are read only by the next step's dilatation
+  // tiles and by the diagnostics, so the step joins it at its end.
   const int n_blk = (lg.abc.n_abc + kAbcWarpsPerBlock - 1) / kAbcWarpsPerBlock;
-  const int n_ent_blk = (lg.abc.n_entries + kAbcWarpsPerBlock - 1) / kAbcWarpsPerBlock;
-  bool late_join = false;  // the G_u/G_v kernel may run on through the force tiles
   if (abc) {
     if (fork) {
       cudaEventRecord(dg.ev_fork[0], st);
       cudaStreamWaitEvent(side, dg.ev_fork[0], 0);
     }
-    if (mode == 0) {
-      k_abc_l2<<<dg.abc_grid, 256, 0, side>>>(lg.abc, p, gth ? 1 : 0, 3 * W);
-      if (fork) cudaEventRecord(dg.ev_join[0], side);
-      if (mark) (*mark)("abc_l2");
+    if (gth) {
+      k_abc_theta<<<n_blk, 256, 0, side>>>(lg.abc, p.th_n, p.th_nm1, p.th_np1);
+      if (mark) (*mark)("abc_theta");
       k++;
-    } else {
-      if (gth) {
-        k_abc_theta<<<n_blk, 256, 0, side>>>(lg.abc, p.th_n, p.th_nm1, p.th_np1);
-        if (mark) (*mark)("abc_theta");
-        k++;
-      }
-      if (mode == 1 || mode == 4) {
-        if (mode == 4 && fork) cudaEventRecord(dg.ev_join[0], side);
-        k_abc_uv_dense<<<n_blk, 256, 0, side>>>(lg.abc, p);
-        if (mark) (*mark)("abc_uv");
-      } else {
-        if (fork) cudaEventRecord(dg.ev_join[0], side);
-        if (mode == 2)
-          k_abc_l2<<<n_ent_blk, 256, 0, side>>>(lg.abc, p, 0, 4096);
-        else
-          k_abc_l2<<<dg.abc_grid, 256, 0, side>>>(lg.abc, p, 0, 3 * W);
-        if (mark) (*mark)("abc_uv");
-      }
-      k++;
-      late_join = mode != 1;
-      if (fork) cudaEventRecord(dg.ev_join[late_join ? 1 : 0], side);
     }
+    if (fork) cudaEventRecord(dg.ev_join[0], side);
+    k_abc_uv_dense<<<n_blk, 256, 0, side>>>(lg.abc, p);
+    if (mark) (*mark)("abc_uv");
+    k++;
+    if (fork) cudaEventRecord(dg.ev_join[1], side);
   }
   for (const auto &gr : dg.groups) {
     LPS_DISPATCH_M(gr.m, launch_theta_group, gr, lg, dg, p, ring_u, gth, st);
@@ -1001,7 +882,7 @@ int enqueue_dense_step(const DenseGeo &dg, const LaunchGeo &lg, const StepPtrs &
     first = false;
     k++;
   }
-  if (abc && fork && late_join) cudaStreamWaitEvent(st, dg.ev_join[1], 0);
+  if (abc && fork) cudaStreamWaitEvent(st, dg.ev_join[1], 0);
   if (mark) (*mark)("force_tiles");
   return k;
 }
