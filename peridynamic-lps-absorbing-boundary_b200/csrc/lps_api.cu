@@ -62,6 +62,8 @@ struct lps_handle {
   int ring_u = 3;             // displacement ring depth: 3 (CSR path) or 4 (dense path)
   double *TH[3] = {};
   double2 *U0 = nullptr, *V0 = nullptr;
+  float2 *U32[2] = {};        // FP32-mixed form: FP32 copies of the predicted level, by step parity
+  float2 *coef32 = nullptr;   // FP32-mixed form: (2(l-m)/m_i, 8mu/m_i) as float2
   // diagnostics
   DiagPartial *partials = nullptr;
   DiagRecord *log = nullptr;
@@ -590,6 +592,12 @@ int build_dense(lps_handle *h, const lps_problem *probs, const std::vector<Latti
   G.xy = d_xy; G.coef = d_coef; G.type = d_type; G.abc_of = d_abc_of; G.blk_inst = d_blk; G.m = d_m;
   G.len = nullptr; G.nbr = nullptr;
   D.tiles = d_tiles;
+  D.fp32 = h->opt.precision == LPS_FP32_MIXED;
+  if (D.fp32) {
+    std::vector<float2> c32(n);
+    for (int c = 0; c < n; c++) c32[c] = make_float2((float)coef[c].x, (float)coef[c].y);
+    if ((st = dev_upload(h, &h->coef32, c32))) return st;
+  }
   if ((st = upload_abc(h, H, total_abc, abc_of))) return st;
   std::map<int, int> done;
   for (int k = 0; k < K; k++) {
@@ -613,7 +621,8 @@ int finish_dense(lps_handle *h) {
   const double2 *coef = h->lg.geo.coef;
   const uint8_t *type = h->lg.geo.type;
   for (auto &gr : D.groups) {
-    const int s = dense_encode_maps(gr, D.pitch, D.total_rows, h->U, h->TH, coef, type, h->err);
+    const int s = dense_encode_maps(gr, D.pitch, D.total_rows, h->U, h->TH, coef, type, D.fp32 ? h->U32 : nullptr,
+                                    h->coef32, h->err);
     if (s) return s;
   }
   LPS_CUDA_TRY(h, cudaStreamCreateWithFlags(&D.side, cudaStreamNonBlocking));
@@ -655,6 +664,8 @@ StepPtrs step_ptrs(lps_handle *h, int64_t n) {
   p.th_n = h->TH[u0];
   p.th_nm1 = h->TH[um];
   p.th_np1 = h->TH[u1];
+  p.u32_np1 = h->U32[(n + 1) % 2];
+  p.u32_np2 = h->U32[n % 2];
   if (h->path == LPS_PATH_DENSE) {
     // the dense step computes G_u concurrently with the predictor that still
     // reads the previous result, so the two alternate by step parity
@@ -804,7 +815,7 @@ int do_reset(lps_handle *h) {
   }
   // dense path: the force pass predicts the next level, so level 1 is
   // predicted here (src/main.cpp:727 with a^0 = 0)
-  if (h->path == LPS_PATH_DENSE) launch_dense_reset_predict(h->lg, h->U0, h->V0, h->U[1], h->VH, st);
+  if (h->path == LPS_PATH_DENSE) launch_dense_reset_predict(h->lg, h->U0, h->V0, h->U[1], h->U32[1], h->VH, st);
   LPS_CUDA_TRY(h, cudaMemsetAsync(h->d_step, 0, sizeof(int), st));
   LPS_CUDA_TRY(h, cudaMemsetAsync(h->log_count, 0, sizeof(int) * h->n_inst, st));
   LPS_CUDA_TRY(h, cudaGetLastError());
@@ -838,6 +849,11 @@ int alloc_state(lps_handle *h) {
       (s = dev_alloc(h, &h->U0, n)) || (s = dev_alloc(h, &h->V0, n)))
     return s;
   LPS_CUDA_TRY(h, cudaMemset(h->VH, 0, sizeof(double2) * n));
+  if (h->dg.fp32)
+    for (int r = 0; r < 2; r++) {
+      if ((s = dev_alloc(h, &h->U32[r], n))) return s;
+      LPS_CUDA_TRY(h, cudaMemset(h->U32[r], 0, sizeof(float2) * n));
+    }
   const int n_part = h->lg.n_node_blocks + (h->n_abc_total + kNodeBlock - 1) / kNodeBlock + 1;
   h->log_capacity = 1024;
   if ((s = dev_alloc(h, &h->partials, n_part)) ||
@@ -915,8 +931,12 @@ int lps_create(const lps_problem *problems, int n_instances, const lps_options *
   lps_options o;
   if (opt) o = *opt; else lps_default_options(&o);
   if (o.max_horizon <= 1) o.max_horizon = 128;
-  if (o.precision != LPS_FP64) {
-    g_create_error = "lps_create: only the FP64 form is available in this build";
+  if (o.precision != LPS_FP64 && o.precision != LPS_FP32_MIXED) {
+    g_create_error = "lps_create: precision must be LPS_FP64 or LPS_FP32_MIXED";
+    return LPS_ERR_INVALID_ARG;
+  }
+  if (o.precision == LPS_FP32_MIXED && o.path == LPS_PATH_CSR) {
+    g_create_error = "lps_create: the FP32-mixed form runs on the dense path only";
     return LPS_ERR_UNSUPPORTED;
   }
   if (o.theta_method != 0 && o.theta_method != 1) {
@@ -979,6 +999,11 @@ int lps_create(const lps_problem *problems, int n_instances, const lps_options *
   int s = LPS_OK;
   std::vector<Lattice> lat;
   const bool dense_ok = o.path != LPS_PATH_CSR && dense_possible(problems, K, h->setup, lat);
+  if (o.precision == LPS_FP32_MIXED && !dense_ok) {
+    h->err = "lps_create: the FP32-mixed form needs the dense path: every instance an exact dx = dy lattice "
+             "with delta/dx in {2,3,4,5,6,8} and no prenotch";
+    return fail(LPS_ERR_UNSUPPORTED);
+  }
   if (o.path == LPS_PATH_DENSE && !dense_ok) {
     h->err = "lps_create: dense path requested but an instance is not an exact dx = dy lattice "
              "with delta/dx in {2,3,4,5,6,8} and no prenotch";

@@ -50,6 +50,8 @@ struct DenseMaps {
   CUtensorMap th[3];      // theta ring
   CUtensorMap coef;       // (2(l-m)/m_i, 8 mu/m_i)
   CUtensorMap type;       // u8 node type
+  CUtensorMap u32[2];     // FP32-mixed form: FP32 predicted displacements, by step parity
+  CUtensorMap coef32;     // FP32-mixed form: coef as float2
 };
 
 struct DenseGroup {
@@ -68,6 +70,7 @@ struct DenseGeo {
   int pitch = 0;
   int total_rows = 0;
   int tile_priority = 0;                       // launch priority of the tile kernels
+  bool fp32 = false;                           // FP32-mixed tile kernels
   cudaStream_t side = nullptr;                 // forked stream for the ABC kernels
   cudaEvent_t ev_fork[2] = {nullptr, nullptr}, ev_join[2] = {nullptr, nullptr};
   int *d_err = nullptr;                        // device wait-timeout flag
@@ -88,19 +91,29 @@ void dense_offsets(int m, std::vector<int> &a, std::vector<int> &b);
 // Per-offset FP64 constants of ratio m for lattice spacing dx (= dy) and
 // horizon delta, into __constant__ memory.
 cudaError_t upload_dense_constants(int m, double dx, double dy, double delta, cudaStream_t st);
-// Encodes the TMA descriptors of group g over the given buffers.
+// Encodes the TMA descriptors of group g over the given buffers (U32 and
+// coef32 only in the FP32-mixed form, else null).
 int dense_encode_maps(DenseGroup &g, int pitch, int total_rows, double2 *const *U, double *const *TH,
-                      const double2 *coef, const uint8_t *type, std::string &err);
+                      const double2 *coef, const uint8_t *type, float2 *const *U32, const float2 *coef32,
+                      std::string &err);
 // Sets shared-memory limits and the persistent grid sizes of each group.
 cudaError_t dense_prepare(DenseGeo &dg);
 
+// FP32-mixed tile kernels (lps_kernels_dense32.cu): shared-memory limits,
+// persistent grids and launches of one group.
+cudaError_t dense32_prepare_group(DenseGroup &gr, int n_sm);
+void launch_theta32_group(const DenseGroup &gr, const LaunchGeo &lg, const DenseGeo &dg, const StepPtrs &p,
+                          int ring_u, bool skip_abc, cudaStream_t st);
+void launch_force32_group(const DenseGroup &gr, const LaunchGeo &lg, const DenseGeo &dg, const StepPtrs &p,
+                          int ring_u, int ring_th, bool abc_on, bool first, int *d_step, cudaStream_t st);
 // One time step: theta tiles || G_theta, [IDW], force tiles; G_u/G_v runs
 // beside both tile passes.
 int enqueue_dense_step(const DenseGeo &dg, const LaunchGeo &lg, const StepPtrs &p, int *d_step,
                        cudaStream_t st, const Mark *mark, int ring_u);
-// Reset helpers: predicted u^1 and vh for every cell from u^0, v^0.
+// Reset helpers: predicted u^1 (and its FP32 copy u32_1 when not null) and
+// vh for every cell from u^0, v^0.
 void launch_dense_reset_predict(const LaunchGeo &lg, const double2 *u0, const double2 *v0, double2 *u1,
-                                double2 *vh, cudaStream_t st);
+                                float2 *u32_1, double2 *vh, cudaStream_t st);
 void launch_theta_dense_init(const DenseGeo &dg, const LaunchGeo &lg, const double2 *u, double *theta,
                              cudaStream_t st);
 void launch_diag_dense(const DenseGeo &dg, const LaunchGeo &lg, const double2 *u, const double2 *v,

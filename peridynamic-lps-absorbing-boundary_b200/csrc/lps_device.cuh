@@ -69,6 +69,8 @@ struct StepPtrs {
   double2 *s_abc;          // G_u result u^{n+1} at ABC nodes, merged next step
   double2 *u_np2;          // dense path: predicted u^{n+2}, written by the force pass
   const double2 *s_prev;   // dense path: G_u result of the previous step (u^n at ABC nodes)
+  float2 *u32_np1;         // FP32-mixed form: FP32 copy of the predicted u^{n+1}
+  float2 *u32_np2;         // FP32-mixed form: FP32 copy of u^{n+2}, written by the force pass
   int th_ring;             // ring index of th_np1
   int pad;
 };

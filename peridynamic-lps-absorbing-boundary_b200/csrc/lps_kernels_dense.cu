@@ -19,55 +19,9 @@
 #include "lps_abc.cuh"
 #include "lps_common.cuh"
 #include "lps_dense.cuh"
+#include "lps_tile.cuh"
 
 namespace lps {
-
-// ---------------------------------------------------------------------------
-// compile-time stencils: {(a, b) != 0 : a^2 + b^2 <= M^2 + M}, enumerated
-// a-major from (-M, -M); offset j and N-1-j are negatives of each other.
-__host__ __device__ constexpr int sten_count(int M) {
-  int n = 0;
-  for (int a = -M; a <= M; a++)
-    for (int b = -M; b <= M; b++)
-      if ((a != 0 || b != 0) && a * a + b * b <= M * M + M) n++;
-  return n;
-}
-__host__ __device__ constexpr int sten_index(int M, int a0, int b0) {
-  int n = 0;
-  for (int a = -M; a <= M; a++)
-    for (int b = -M; b <= M; b++)
-      if ((a != 0 || b != 0) && a * a + b * b <= M * M + M) {
-        if (a == a0 && b == b0) return n;
-        n++;
-      }
-  return -1;
-}
-// largest |a| with a^2 + b^2 <= M^2 + M
-__host__ __device__ constexpr int amax(int M, int b) {
-  int A = 0;
-  while ((A + 1) * (A + 1) + b * b <= M * M + M) A++;
-  return A;
-}
-
-template <int M>
-struct Sten {
-  static constexpr int N = sten_count(M);
-  int a[N], b[N];
-};
-
-template <int M>
-__host__ __device__ constexpr Sten<M> make_sten() {
-  Sten<M> s{};
-  int n = 0;
-  for (int a = -M; a <= M; a++)
-    for (int b = -M; b <= M; b++)
-      if ((a != 0 || b != 0) && a * a + b * b <= M * M + M) {
-        s.a[n] = a;
-        s.b[n] = b;
-        n++;
-      }
-  return s;
-}
 
 // Per-offset constants, 7 rows of N doubles per supported M:
 //   0: xi_hat_x  1: xi_hat_y  2: |xi|  3: g_x = beta dV xi_hat_x
@@ -102,17 +56,6 @@ static void offsets_of(std::vector<int> &a, std::vector<int> &b) {
   b.assign(s.b, s.b + Sten<M>::N);
 }
 
-#define LPS_DISPATCH_M(m, FN, ...)      \
-  switch (m) {                          \
-    case 2: FN<2>(__VA_ARGS__); break;  \
-    case 3: FN<3>(__VA_ARGS__); break;  \
-    case 4: FN<4>(__VA_ARGS__); break;  \
-    case 5: FN<5>(__VA_ARGS__); break;  \
-    case 6: FN<6>(__VA_ARGS__); break;  \
-    case 8: FN<8>(__VA_ARGS__); break;  \
-    default: break;                     \
-  }
-
 void dense_offsets(int m, std::vector<int> &a, std::vector<int> &b) {
   a.clear();
   b.clear();
@@ -146,98 +89,6 @@ cudaError_t upload_dense_constants(int m, double dx, double dy, double delta, cu
 }
 
 // ---------------------------------------------------------------------------
-// staged region geometry
-template <int M>
-struct Region {
-  static constexpr int RR = kTileRows + 2 * M;   // staged rows
-  static constexpr int RC = kTileCols + 2 * M;   // staged columns (f64 boxes)
-  static constexpr int RT = 48;                  // staged columns of the u8 box (x16 bytes)
-  static constexpr int CELLS = RR * RC;
-  static_assert(RC <= RT, "type box narrower than the region");
-  static constexpr int U_BYTES = CELLS * 16;
-  static constexpr int TH_BYTES = CELLS * 8;
-  static constexpr int CO_BYTES = CELLS * 16;
-  static constexpr int TY_BYTES = RR * RT;
-  static constexpr int align128(int x) { return (x + 127) / 128 * 128; }
-  // every TMA destination starts on a 128-byte boundary
-  // theta stage: u | type
-  static constexpr int T_TY = align128(U_BYTES);
-  static constexpr int THETA_STAGE = align128(T_TY + TY_BYTES);
-  static constexpr int THETA_TX = U_BYTES + TY_BYTES;
-  // force stage: u | th | coef | type
-  static constexpr int F_TH = align128(U_BYTES);
-  static constexpr int F_CO = align128(F_TH + TH_BYTES);
-  static constexpr int F_TY = align128(F_CO + CO_BYTES);
-  static constexpr int FORCE_STAGE = align128(F_TY + TY_BYTES);
-  static constexpr int FORCE_TX = U_BYTES + TH_BYTES + CO_BYTES + TY_BYTES;
-  static constexpr int THETA_SMEM = 2 * THETA_STAGE + 64;
-  static constexpr int FORCE_SMEM = 2 * FORCE_STAGE + 64;
-};
-
-// ---- TMA / mbarrier primitives (inline PTX) --------------------------------
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_fence_init() {
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y, uint64_t *bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
-          smem_u32(dst)),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
-      : "memory");
-}
-__device__ __forceinline__ void fence_proxy_async_smem() {
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-
-// Bounded wait on a transaction barrier: gives up after ~2 s (clock64) or
-// 2^26 polls, whichever comes first, and raises the error flag.
-constexpr int kErrWaitTimeout = 1;
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, int *err) {
-  if (mbar_try_wait(bar, parity)) return true;
-  const long long t0 = clock64();
-  for (int it = 0; it < (1 << 26); it++) {
-    if (mbar_try_wait(bar, parity)) return true;
-    if (clock64() - t0 > 4000000000LL) break;
-  }
-  atomicExch(err, kErrWaitTimeout);
-  return false;
-}
-
-// Dynamic tile scheduler of the persistent tile kernels: a CTA takes its next
-// tile from a counter, so a CTA that becomes resident late (its SM still runs
-// blocks of the concurrent absorbing-boundary kernel) takes fewer tiles instead
-// of stretching the launch.  sched[0] is the next tile, sched[1] counts
-// finished CTAs; the last CTA to finish rewinds both for the next launch.
-__device__ __forceinline__ int sched_next(int *sched) { return atomicAdd(sched, 1); }
-
-__device__ __forceinline__ void sched_finish(int *sched) {
-  __threadfence();
-  if (atomicAdd(sched + 1, 1) == (int)gridDim.x - 1) {
-    sched[0] = 0;
-    sched[1] = 0;
-  }
-}
-
-// ---------------------------------------------------------------------------
 // Tile compute.  A thread owns cells (r0, c) and (r0 + 1, c); for every pair
 // of opposite offsets (a, b) / (-a, -b) it reads the two staged neighbours of
 // each cell -- the row-(r0+1) reads of one offset are the row-r0 reads of the
@@ -248,48 +99,40 @@ __device__ __forceinline__ void sched_finish(int *sched) {
 // theta, B = 8 mu / m (:857-869).  Masked tiles (near the domain edge) use the
 // same pairs with absent neighbours zeroed: u = A = B = 0 there, and the
 // owned node's own terms are weighted by which side is present.
-template <int M>
-__device__ __forceinline__ int QI(int r, int c) {
-  return (r + M) * Region<M>::RC + (c + M);
-}
-
 template <int M, bool FULL>
 __device__ __forceinline__ void theta_tile(const double2 *__restrict__ su, const uint8_t *__restrict__ sty, int r0,
                                            int c, double th[2]) {
   using R = Region<M>;
   const double2 ui0 = su[QI<M>(r0, c)], ui1 = su[QI<M>(r0 + 1, c)];
   double s00 = 0.0, s01 = 0.0, s10 = 0.0, s11 = 0.0;
+  for_each_pair<M>(
+      [&](auto ac, auto bc) {
+        constexpr int a = decltype(ac)::value, b = decltype(bc)::value;
+        constexpr int j = sten_index(M, a, b);
+        const double cx = SC<M>(5, j), cy = SC<M>(6, j);
 #pragma unroll
-  for (int b = 0; b <= M; b++) {
-    const int A = amax(M, b);
-#pragma unroll
-    for (int a = -A; a <= A; a++) {
-      if (b == 0 && a <= 0) continue;
-      const int j = sten_index(M, a, b);
-      const double cx = SC<M>(5, j), cy = SC<M>(6, j);
-#pragma unroll
-      for (int k = 0; k < 2; k++) {
-        const int r = r0 + k;
-        const double2 up = su[QI<M>(r + a, c + b)], um = su[QI<M>(r - a, c - b)];
-        double dx = up.x - um.x, dy = up.y - um.y;
-        if (!FULL) {
-          // absent neighbours hold u = 0; restore the -u_i of the present side
-          const double mp = (sty[(r + a + M) * R::RT + c + b + M] & kExists) ? 1.0 : 0.0;
-          const double mm = (sty[(r - a + M) * R::RT + c - b + M] & kExists) ? 1.0 : 0.0;
-          const double2 ui = k == 0 ? ui0 : ui1;
-          dx = fma(mm - mp, ui.x, dx);
-          dy = fma(mm - mp, ui.y, dy);
+        for (int k = 0; k < 2; k++) {
+          const int r = r0 + k;
+          const double2 up = su[QI<M>(r + a, c + b)], um = su[QI<M>(r - a, c - b)];
+          double dx = up.x - um.x, dy = up.y - um.y;
+          if (!FULL) {
+            // absent neighbours hold u = 0; restore the -u_i of the present side
+            const double mp = (sty[(r + a + M) * R::RT + c + b + M] & kExists) ? 1.0 : 0.0;
+            const double mm = (sty[(r - a + M) * R::RT + c - b + M] & kExists) ? 1.0 : 0.0;
+            const double2 ui = k == 0 ? ui0 : ui1;
+            dx = fma(mm - mp, ui.x, dx);
+            dy = fma(mm - mp, ui.y, dy);
+          }
+          if (k == 0) {
+            s00 = fma(cx, dx, s00);
+            s01 = fma(cy, dy, s01);
+          } else {
+            s10 = fma(cx, dx, s10);
+            s11 = fma(cy, dy, s11);
+          }
         }
-        if (k == 0) {
-          s00 = fma(cx, dx, s00);
-          s01 = fma(cy, dy, s01);
-        } else {
-          s10 = fma(cx, dx, s10);
-          s11 = fma(cy, dy, s11);
-        }
-      }
-    }
-  }
+      },
+      [](auto) {});
   th[0] = s00 + s01;
   th[1] = s10 + s11;
 }
@@ -304,41 +147,38 @@ __device__ __forceinline__ void force_tile(const double2 *__restrict__ su, const
     ui[k] = su[QI<M>(r0 + k, c)];
     ab_i[k] = sab[QI<M>(r0 + k, c)];
   }
+  for_each_pair<M>(
+      [&](auto ac, auto bc) {
+        constexpr int a = decltype(ac)::value, b = decltype(bc)::value;
+        constexpr int j = sten_index(M, a, b);
+        const double hx = SC<M>(0, j), hy = SC<M>(1, j), L = SC<M>(2, j);
+        const double gx = SC<M>(3, j), gy = SC<M>(4, j);
 #pragma unroll
-  for (int b = 0; b <= M; b++) {
-    const int A = amax(M, b);
-#pragma unroll
-    for (int a = -A; a <= A; a++) {
-      if (b == 0 && a <= 0) continue;
-      const int j = sten_index(M, a, b);
-      const double hx = SC<M>(0, j), hy = SC<M>(1, j), L = SC<M>(2, j);
-      const double gx = SC<M>(3, j), gy = SC<M>(4, j);
-#pragma unroll
-      for (int k = 0; k < 2; k++) {
-        const int r = r0 + k;
-        const int qp = QI<M>(r + a, c + b), qm = QI<M>(r - a, c - b);
-        const double2 up = su[qp], um = su[qm], abp = sab[qp], abm = sab[qm];
-        const double e1 = hx * (up.x - ui[k].x) + hy * (up.y - ui[k].y);
-        const double e2 = hx * (ui[k].x - um.x) + hy * (ui[k].y - um.y);
-        double T, wp, wm;
-        if (FULL) {
-          T = (abp.x - abm.x) * L;
-          wp = ab_i[k].y + abp.y;
-          wm = ab_i[k].y + abm.y;
-        } else {
-          // a valid neighbour has B > 0; an absent one has A = B = 0
-          const double mp = abp.y > 0.0 ? 1.0 : 0.0, mm = abm.y > 0.0 ? 1.0 : 0.0;
-          T = fma(mp - mm, ab_i[k].x, abp.x - abm.x) * L;
-          wp = fma(mp, ab_i[k].y, abp.y);
-          wm = fma(mm, ab_i[k].y, abm.y);
+        for (int k = 0; k < 2; k++) {
+          const int r = r0 + k;
+          const int qp = QI<M>(r + a, c + b), qm = QI<M>(r - a, c - b);
+          const double2 up = su[qp], um = su[qm], abp = sab[qp], abm = sab[qm];
+          const double e1 = hx * (up.x - ui[k].x) + hy * (up.y - ui[k].y);
+          const double e2 = hx * (ui[k].x - um.x) + hy * (ui[k].y - um.y);
+          double T, wp, wm;
+          if (FULL) {
+            T = (abp.x - abm.x) * L;
+            wp = ab_i[k].y + abp.y;
+            wm = ab_i[k].y + abm.y;
+          } else {
+            // a valid neighbour has B > 0; an absent one has A = B = 0
+            const double mp = abp.y > 0.0 ? 1.0 : 0.0, mm = abm.y > 0.0 ? 1.0 : 0.0;
+            T = fma(mp - mm, ab_i[k].x, abp.x - abm.x) * L;
+            wp = fma(mp, ab_i[k].y, abp.y);
+            wm = fma(mm, ab_i[k].y, abm.y);
+          }
+          T = fma(wp, e1, T);
+          T = fma(-wm, e2, T);
+          F0[k] = fma(T, gx, F0[k]);
+          F1[k] = fma(T, gy, F1[k]);
         }
-        T = fma(wp, e1, T);
-        T = fma(-wm, e2, T);
-        F0[k] = fma(T, gx, F0[k]);
-        F1[k] = fma(T, gy, F1[k]);
-      }
-    }
-  }
+      },
+      [](auto) {});
 #pragma unroll
   for (int k = 0; k < 2; k++) F[k] = make_double2(F0[k], F1[k]);
 }
@@ -691,11 +531,12 @@ __global__ void __launch_bounds__(kNodeBlock)
 
 // u^1 = u^0 + dt (v^0 + dt/2 a^0) with a^0 = 0, and vh = v^0, src/main.cpp:727.
 __global__ void __launch_bounds__(256) k_dense_reset_predict(Geo g, const double2 *u0, const double2 *v0,
-                                                              double2 *u1, double2 *vh) {
+                                                              double2 *u1, float2 *u32_1, double2 *vh) {
   const size_t cell = (size_t)blockIdx.x * 256 + threadIdx.x;
   if (cell >= (size_t)g.n_total) return;
   if (!(g.type[cell] & kExists)) {
     u1[cell] = make_double2(0.0, 0.0);
+    if (u32_1) u32_1[cell] = make_float2(0.f, 0.f);
     vh[cell] = make_double2(0.0, 0.0);
     return;
   }
@@ -707,6 +548,7 @@ __global__ void __launch_bounds__(256) k_dense_reset_predict(Geo g, const double
   up.x = u.x + P.dt * h.x;
   up.y = u.y + P.dt * h.y;
   u1[cell] = up;
+  if (u32_1) u32_1[cell] = make_float2((float)up.x, (float)up.y);
   vh[cell] = h;
 }
 
@@ -748,7 +590,10 @@ cudaError_t dense_prepare(DenseGeo &dg) {
   dg.tile_priority = greatest;  // tile CTAs are dispatched ahead of the ABC kernel's blocks
   for (auto &gr : dg.groups) {
     cudaError_t e = cudaErrorInvalidValue;
-    LPS_DISPATCH_M(gr.m, prepare_dispatch, gr, n_sm, &e);
+    if (dg.fp32)
+      e = dense32_prepare_group(gr, n_sm);
+    else
+      LPS_DISPATCH_M(gr.m, prepare_dispatch, gr, n_sm, &e);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
@@ -782,9 +627,16 @@ bool encode(CUtensorMap *map, CUtensorMapDataType dt, size_t elem, const void *b
 
 template <int M>
 void encode_m(DenseGroup &g, int pitch, int rows, double2 *const *U, double *const *TH, const double2 *coef,
-              const uint8_t *type, bool *ok) {
+              const uint8_t *type, float2 *const *U32, const float2 *coef32, bool *ok) {
   using R = Region<M>;
   bool good = true;
+  if (U32) {
+    for (int r = 0; r < 2; r++)
+      good &= encode(&g.maps.u32[r], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, U32[r], 2ull * pitch, rows, 2 * R::RC,
+                     R::RR);
+    good &= encode(&g.maps.coef32, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, coef32, 2ull * pitch, rows, 2 * R::RC,
+                   R::RR);
+  }
   for (int r = 0; r < kUring; r++)
     good &= encode(&g.maps.u[r], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, U[r], 2ull * pitch, rows, 2 * R::RC, R::RR);
   for (int r = 0; r < 3; r++)
@@ -796,9 +648,10 @@ void encode_m(DenseGroup &g, int pitch, int rows, double2 *const *U, double *con
 }  // namespace
 
 int dense_encode_maps(DenseGroup &g, int pitch, int total_rows, double2 *const *U, double *const *TH,
-                      const double2 *coef, const uint8_t *type, std::string &err) {
+                      const double2 *coef, const uint8_t *type, float2 *const *U32, const float2 *coef32,
+                      std::string &err) {
   bool ok = false;
-  LPS_DISPATCH_M(g.m, encode_m, g, pitch, total_rows, U, TH, coef, type, &ok);
+  LPS_DISPATCH_M(g.m, encode_m, g, pitch, total_rows, U, TH, coef, type, U32, coef32, &ok);
   if (!ok) {
     err = "cuTensorMapEncodeTiled failed for the dense layout";
     return LPS_ERR_CUDA;
@@ -865,7 +718,10 @@ int enqueue_dense_step(const DenseGeo &dg, const LaunchGeo &lg, const StepPtrs &
     if (fork) cudaEventRecord(dg.ev_join[1], side);
   }
   for (const auto &gr : dg.groups) {
-    LPS_DISPATCH_M(gr.m, launch_theta_group, gr, lg, dg, p, ring_u, gth, st);
+    if (dg.fp32)
+      launch_theta32_group(gr, lg, dg, p, ring_u, gth, st);
+    else
+      LPS_DISPATCH_M(gr.m, launch_theta_group, gr, lg, dg, p, ring_u, gth, st);
     k++;
   }
   if (abc && fork) cudaStreamWaitEvent(st, dg.ev_join[0], 0);
@@ -878,7 +734,10 @@ int enqueue_dense_step(const DenseGeo &dg, const LaunchGeo &lg, const StepPtrs &
   // pass 2: force tiles
   bool first = true;
   for (const auto &gr : dg.groups) {
-    LPS_DISPATCH_M(gr.m, launch_force_group, gr, lg, dg, p, ring_u, rth, abc, first, d_step, st);
+    if (dg.fp32)
+      launch_force32_group(gr, lg, dg, p, ring_u, rth, abc, first, d_step, st);
+    else
+      LPS_DISPATCH_M(gr.m, launch_force_group, gr, lg, dg, p, ring_u, rth, abc, first, d_step, st);
     first = false;
     k++;
   }
@@ -888,8 +747,8 @@ int enqueue_dense_step(const DenseGeo &dg, const LaunchGeo &lg, const StepPtrs &
 }
 
 void launch_dense_reset_predict(const LaunchGeo &lg, const double2 *u0, const double2 *v0, double2 *u1,
-                                double2 *vh, cudaStream_t st) {
-  k_dense_reset_predict<<<lg.n_node_blocks, 256, 0, st>>>(lg.geo, u0, v0, u1, vh);
+                                float2 *u32_1, double2 *vh, cudaStream_t st) {
+  k_dense_reset_predict<<<lg.n_node_blocks, 256, 0, st>>>(lg.geo, u0, v0, u1, u32_1, vh);
 }
 
 void launch_theta_dense_init(const DenseGeo &, const LaunchGeo &lg, const double2 *u, double *theta,

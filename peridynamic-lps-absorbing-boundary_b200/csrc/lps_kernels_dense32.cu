@@ -1,0 +1,410 @@
+// lps_kernels_dense32.cu -- FP32-mixed form of the dense tile kernels, sm_100a.
+//
+// Same two persistent passes as the FP64 form (lps_kernels_dense.cu), with
+// the bond arithmetic in FP32:
+//   k_theta32<M>   dilatation (src/main.cpp:736-761) from an FP32 copy of the
+//                  predicted displacements
+//   k_force32<M>   force (:821-874) in FP32; corrector (:922-925) and the next
+//                  predictor (:725-728) in FP64, which also writes the FP32
+//                  copy of the next predicted level
+// Kept in FP64: the displacement / velocity / acceleration state and its
+// Verlet update, theta storage, the absorbing-boundary operators (their own
+// kernels are shared with the FP64 form) and the diagnostics.
+//
+// Per-offset constants are compile-time values in lattice units: on the dense
+// path dx = dy and delta = m dx, so with xi = dx (a, b), r = |(a, b)|,
+//   beta = 1 (r <= m - 1/2), m + 1/2 - r (r <= m + 1/2), 0    (:98-105)
+//   theta_i = (2 dx^3 / m_i) sum beta (a, b) . eta
+//   F_i     = dx^2 sum beta xi_hat [ (A'+ - A'-) r + (B_i + B+) e+ - (B_i + B-) e- ]
+// with A' = dx (2(l-m)/m) theta.  Each stencil column's partial sum is added
+// to the cell's total with Kahan compensation.
+#include <cmath>
+
+#include "lps_common.cuh"
+#include "lps_dense.cuh"
+#include "lps_tile.cuh"
+
+namespace lps {
+
+// Square root by Newton's iteration, for compile-time tables only.
+__host__ __device__ constexpr double ct_sqrt(double x) {
+  double r = x > 1.0 ? x : 1.0;
+  for (int i = 0; i < 100; i++) r = 0.5 * (r + x / r);
+  return r;
+}
+
+// Per-offset constants in lattice units, evaluated by the compiler for each
+// (a, b) of the unrolled stencil.
+enum StenQ { kHx, kHy, kR, kGx, kGy, kWx, kWy };
+
+__host__ __device__ constexpr float sten_q(int Q, int M, int a, int b) {
+  const double r = ct_sqrt((double)(a * a + b * b));
+  const double beta = r <= M - 0.5 ? 1.0 : (r <= M + 0.5 ? M + 0.5 - r : 0.0);
+  switch (Q) {
+    case kHx: return (float)(a / r);           // xi_hat
+    case kHy: return (float)(b / r);
+    case kR: return (float)r;                  // |xi| / dx
+    case kGx: return (float)(beta * a / r);    // beta xi_hat
+    case kGy: return (float)(beta * b / r);
+    case kWx: return (float)(beta * a);        // beta (a, b)
+    default: return (float)(beta * b);
+  }
+}
+
+template <int M>
+using Region32 = Region<M, 8, 8>;
+
+// s + x with Kahan's running compensation c (the estimate is s - c).
+__device__ __forceinline__ void kahan_add(float &s, float &c, float x) {
+  const float y = x - c;
+  const float t = s + y;
+  c = (t - s) - y;
+  s = t;
+}
+
+// Thread owns cells (r0, c) and (r0 + 1, c), as in the FP64 form.
+template <int M, bool FULL>
+__device__ __forceinline__ void theta_tile32(const float2 *__restrict__ su, const uint8_t *__restrict__ sty, int r0,
+                                             int c, float th[2]) {
+  using R = Region32<M>;
+  const float2 ui0 = su[QI<M>(r0, c)], ui1 = su[QI<M>(r0 + 1, c)];
+  float S[2] = {0.f, 0.f}, C[2] = {0.f, 0.f}, part[2] = {0.f, 0.f};
+  for_each_pair<M>(
+      [&](auto ac, auto bc) {
+        constexpr int a = decltype(ac)::value, b = decltype(bc)::value;
+        constexpr float wx = sten_q(kWx, M, a, b), wy = sten_q(kWy, M, a, b);
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+          const int r = r0 + k;
+          const float2 up = su[QI<M>(r + a, c + b)], um = su[QI<M>(r - a, c - b)];
+          float dx = up.x - um.x, dy = up.y - um.y;
+          if (!FULL) {
+            // absent neighbours hold u = 0; restore the -u_i of the present side
+            const float mp = (sty[(r + a + M) * R::RT + c + b + M] & kExists) ? 1.f : 0.f;
+            const float mm = (sty[(r - a + M) * R::RT + c - b + M] & kExists) ? 1.f : 0.f;
+            const float2 ui = k == 0 ? ui0 : ui1;
+            dx = fmaf(mm - mp, ui.x, dx);
+            dy = fmaf(mm - mp, ui.y, dy);
+          }
+          part[k] = fmaf(wx, dx, part[k]);
+          part[k] = fmaf(wy, dy, part[k]);
+        }
+      },
+      [&](auto) {
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+          kahan_add(S[k], C[k], part[k]);
+          part[k] = 0.f;
+        }
+      });
+  th[0] = S[0] - C[0];
+  th[1] = S[1] - C[1];
+}
+
+template <int M, bool FULL>
+__device__ __forceinline__ void force_tile32(const float2 *__restrict__ su, const float2 *__restrict__ sab, int r0,
+                                             int c, float F[2][2]) {
+  float2 ui[2], ab_i[2];
+  float S0[2] = {0.f, 0.f}, C0[2] = {0.f, 0.f}, S1[2] = {0.f, 0.f}, C1[2] = {0.f, 0.f};
+  float p0[2] = {0.f, 0.f}, p1[2] = {0.f, 0.f};
+#pragma unroll
+  for (int k = 0; k < 2; k++) {
+    ui[k] = su[QI<M>(r0 + k, c)];
+    ab_i[k] = sab[QI<M>(r0 + k, c)];
+  }
+  for_each_pair<M>(
+      [&](auto ac, auto bc) {
+        constexpr int a = decltype(ac)::value, b = decltype(bc)::value;
+        constexpr float hx = sten_q(kHx, M, a, b), hy = sten_q(kHy, M, a, b), L = sten_q(kR, M, a, b);
+        constexpr float gx = sten_q(kGx, M, a, b), gy = sten_q(kGy, M, a, b);
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+          const int r = r0 + k;
+          const int qp = QI<M>(r + a, c + b), qm = QI<M>(r - a, c - b);
+          const float2 up = su[qp], um = su[qm], abp = sab[qp], abm = sab[qm];
+          const float e1 = fmaf(hx, up.x - ui[k].x, hy * (up.y - ui[k].y));
+          const float e2 = fmaf(hx, ui[k].x - um.x, hy * (ui[k].y - um.y));
+          float T, wp, wm;
+          if (FULL) {
+            T = (abp.x - abm.x) * L;
+            wp = ab_i[k].y + abp.y;
+            wm = ab_i[k].y + abm.y;
+          } else {
+            // a valid neighbour has B > 0; an absent one has A = B = 0
+            const float mp = abp.y > 0.f ? 1.f : 0.f, mm = abm.y > 0.f ? 1.f : 0.f;
+            T = fmaf(mp - mm, ab_i[k].x, abp.x - abm.x) * L;
+            wp = fmaf(mp, ab_i[k].y, abp.y);
+            wm = fmaf(mm, ab_i[k].y, abm.y);
+          }
+          T = fmaf(wp, e1, T);
+          T = fmaf(-wm, e2, T);
+          p0[k] = fmaf(T, gx, p0[k]);
+          p1[k] = fmaf(T, gy, p1[k]);
+        }
+      },
+      [&](auto) {
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+          kahan_add(S0[k], C0[k], p0[k]);
+          kahan_add(S1[k], C1[k], p1[k]);
+          p0[k] = p1[k] = 0.f;
+        }
+      });
+#pragma unroll
+  for (int k = 0; k < 2; k++) {
+    F[k][0] = S0[k] - C0[k];
+    F[k][1] = S1[k] - C1[k];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Predicted displacements (FP32 copy) -> dilatation, persistent over tiles.
+template <int M>
+__global__ void __launch_bounds__(kTileThreads, 2)
+    k_theta32(const __grid_constant__ CUtensorMap map_u, const __grid_constant__ CUtensorMap map_type, Geo g,
+              const DenseTile *__restrict__ tiles, int tile_begin, int n_tiles, StepPtrs p, int pitch, int skip_abc,
+              int *sched, int *err) {
+  using R = Region32<M>;
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem + 2 * R::THETA_STAGE);
+  int *s_tile = reinterpret_cast<int *>(bar + 2);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (*(volatile int *)err) return;  // an earlier wait timed out: do nothing
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_fence_init();
+    s_tile[0] = sched_next(sched);
+  }
+  __syncthreads();
+  auto issue = [&](int stage, int tile) {
+    const DenseTile t = tiles[tile_begin + tile];
+    unsigned char *base = smem + stage * R::THETA_STAGE;
+    mbar_expect_tx(&bar[stage], R::THETA_TX);
+    tma_load_2d(base, &map_u, 2 * t.col, t.row, &bar[stage]);
+    tma_load_2d(base + R::T_TY, &map_type, t.col, t.row, &bar[stage]);
+  };
+  int tile = s_tile[0];
+  if (tid == 0 && tile < n_tiles) issue(0, tile);
+  for (int it = 0; tile < n_tiles; it++, tile = s_tile[it & 1]) {
+    const int stage = it & 1;
+    if (tid == 0) {
+      const int nx = sched_next(sched);
+      s_tile[stage ^ 1] = nx;
+      if (nx < n_tiles) issue(stage ^ 1, nx);
+    }
+    const DenseTile t = tiles[tile_begin + tile];
+    const InstParams &P = c_inst[t.inst];
+    float2 *su = reinterpret_cast<float2 *>(smem + stage * R::THETA_STAGE);
+    uint8_t *sty = reinterpret_cast<uint8_t *>(smem + stage * R::THETA_STAGE + R::T_TY);
+    const int r0 = 2 * warp;
+    const size_t cell0 = (size_t)(t.row + M + r0) * pitch + t.col + M + lane;
+    const double mi0 = g.m[cell0], mi1 = g.m[cell0 + pitch];
+    if (!mbar_wait_bounded(&bar[stage], (it >> 1) & 1, err)) return;
+    if (t.flags & kTileAbc) {
+      // ABC nodes: u^n from the last G_u, predicted here in FP64 (src/main.cpp:727)
+      for (int q = tid; q < R::CELLS; q += kTileThreads) {
+        const int rr = q / R::RC, cc = q - rr * R::RC;
+        if (!(sty[rr * R::RT + cc] & kActiveAbc)) continue;
+        const size_t cell = (size_t)(t.row + rr) * pitch + t.col + cc;
+        const double2 u = p.s_prev[g.abc_of[cell]], v = p.v_n[cell], a = p.a_n[cell];
+        double2 vh, up;
+        vh.x = v.x + P.half_dt * a.x;
+        vh.y = v.y + P.half_dt * a.y;
+        up.x = u.x + P.dt * vh.x;
+        up.y = u.y + P.dt * vh.y;
+        const float2 up32 = make_float2((float)up.x, (float)up.y);
+        su[q] = up32;
+        if (rr >= M && rr < M + kTileRows && cc >= M && cc < M + kTileCols) {
+          p.u_np1[cell] = up;
+          p.u32_np1[cell] = up32;
+          p.vh[cell] = vh;
+          p.u_n[cell] = u;
+        }
+      }
+      __syncthreads();
+    }
+    float th[2];
+    if (t.flags & kTileFull)
+      theta_tile32<M, true>(su, sty, r0, lane, th);
+    else
+      theta_tile32<M, false>(su, sty, r0, lane, th);
+    const double scale = 2.0 * P.dx * P.dy * P.dx;
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+      const uint8_t ty = sty[(r0 + k + M) * R::RT + lane + M];
+      if (!(ty & kExists)) continue;
+      if (skip_abc && (ty & kActiveAbc)) continue;  // the G_theta kernel writes it
+      const double mi = k == 0 ? mi0 : mi1;
+      p.th_np1[cell0 + (size_t)k * pitch] = (mi > 0.0) ? (scale / mi) * (double)th[k] : 0.0;
+    }
+    fence_proxy_async_smem();
+    __syncthreads();  // the stage is refilled at the start of the next-but-one iteration
+  }
+  if (tid == 0) sched_finish(sched);
+}
+
+// ---------------------------------------------------------------------------
+// Force (FP32) + corrector + next predictor (FP64), persistent over tiles.
+// After the copy lands, (theta, coef) become (A', B) = (dx 2(l-m)/m theta,
+// 8 mu/m) in the coef slot; absent neighbours and m <= 0 get A' = B = 0.
+template <int M>
+__global__ void __launch_bounds__(kTileThreads, 2)
+    k_force32(const __grid_constant__ CUtensorMap map_u, const __grid_constant__ CUtensorMap map_th,
+              const __grid_constant__ CUtensorMap map_coef, const __grid_constant__ CUtensorMap map_type, Geo g,
+              const DenseTile *__restrict__ tiles, int tile_begin, int n_tiles, StepPtrs p, int pitch, int abc_on,
+              int bump_step, int *d_step, int *sched, int *err) {
+  using R = Region32<M>;
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem + 2 * R::FORCE_STAGE);
+  int *s_tile = reinterpret_cast<int *>(bar + 2);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (*(volatile int *)err) return;  // an earlier wait timed out: do nothing
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_fence_init();
+    if (bump_step && blockIdx.x == 0) *d_step += 1;
+    s_tile[0] = sched_next(sched);
+  }
+  __syncthreads();
+  auto issue = [&](int stage, int tile) {
+    const DenseTile t = tiles[tile_begin + tile];
+    unsigned char *base = smem + stage * R::FORCE_STAGE;
+    mbar_expect_tx(&bar[stage], R::FORCE_TX);
+    tma_load_2d(base, &map_u, 2 * t.col, t.row, &bar[stage]);
+    tma_load_2d(base + R::F_TH, &map_th, t.col, t.row, &bar[stage]);
+    tma_load_2d(base + R::F_CO, &map_coef, 2 * t.col, t.row, &bar[stage]);
+    tma_load_2d(base + R::F_TY, &map_type, t.col, t.row, &bar[stage]);
+  };
+  int tile = s_tile[0];
+  if (tid == 0 && tile < n_tiles) issue(0, tile);
+  for (int it = 0; tile < n_tiles; it++, tile = s_tile[it & 1]) {
+    const int stage = it & 1;
+    if (tid == 0) {
+      const int nx = sched_next(sched);
+      s_tile[stage ^ 1] = nx;
+      if (nx < n_tiles) issue(stage ^ 1, nx);
+    }
+    const DenseTile t = tiles[tile_begin + tile];
+    const InstParams &P = c_inst[t.inst];
+    unsigned char *base = smem + stage * R::FORCE_STAGE;
+    const float2 *su = reinterpret_cast<const float2 *>(base);
+    const double *sth = reinterpret_cast<const double *>(base + R::F_TH);
+    float2 *sab = reinterpret_cast<float2 *>(base + R::F_CO);
+    const uint8_t *sty = reinterpret_cast<const uint8_t *>(base + R::F_TY);
+    const int r0 = 2 * warp;
+    const size_t cell0 = (size_t)(t.row + M + r0) * pitch + t.col + M + lane;
+    const double2 vh0 = p.vh[cell0], vh1 = p.vh[cell0 + pitch];
+    if (!mbar_wait_bounded(&bar[stage], (it >> 1) & 1, err)) return;
+    const float dxf = (float)P.dx;
+    for (int q = tid; q < R::CELLS; q += kTileThreads) {
+      const int rr = q / R::RC, cc = q - rr * R::RC;
+      const float2 co = sab[q];
+      const bool valid = (sty[rr * R::RT + cc] & kExists) && co.y >= 0.f;
+      sab[q] = valid ? make_float2(co.x * (float)sth[q] * dxf, co.y) : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    float F[2][2];
+    if (t.flags & kTileFull)
+      force_tile32<M, true>(su, sab, r0, lane, F);
+    else
+      force_tile32<M, false>(su, sab, r0, lane, F);
+    const double scale = P.dx * P.dy / P.rho;
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+      const uint8_t ty = sty[(r0 + k + M) * R::RT + lane + M];
+      if (!(ty & kExists)) continue;
+      const size_t cell = cell0 + (size_t)k * pitch;
+      const bool valid = sab[QI<M>(r0 + k, lane)].y > 0.f;  // m_i > 0 (:827-831)
+      const double2 acc =
+          valid ? make_double2((double)F[k][0] * scale, (double)F[k][1] * scale) : make_double2(0.0, 0.0);
+      p.a_np1[cell] = acc;
+      if (abc_on && (ty & kActiveAbc)) continue;  // G_v writes v; the next theta kernel predicts u
+      // corrector (:924) then the next predictor (:727), FP64
+      const double2 vh = k == 0 ? vh0 : vh1;
+      double2 v, vh2, un;
+      v.x = vh.x + P.half_dt * acc.x;
+      v.y = vh.y + P.half_dt * acc.y;
+      vh2.x = v.x + P.half_dt * acc.x;
+      vh2.y = v.y + P.half_dt * acc.y;
+      const double2 u = p.u_np1[cell];
+      un.x = u.x + P.dt * vh2.x;
+      un.y = u.y + P.dt * vh2.y;
+      p.v_np1[cell] = v;
+      p.vh[cell] = vh2;
+      p.u_np2[cell] = un;
+      p.u32_np2[cell] = make_float2((float)un.x, (float)un.y);
+    }
+    fence_proxy_async_smem();
+    __syncthreads();
+  }
+  if (tid == 0) sched_finish(sched);
+}
+
+// ---------------------------------------------------------------------------
+// host side
+template <int M>
+static void prepare32_m(DenseGroup &gr, int n_sm, cudaError_t *out) {
+  using R = Region32<M>;
+  cudaError_t e;
+  *out = cudaSuccess;
+  if ((e = cudaFuncSetAttribute(k_theta32<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, R::THETA_SMEM)) ||
+      (e = cudaFuncSetAttribute(k_force32<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, R::FORCE_SMEM))) {
+    *out = e;
+    return;
+  }
+  int bt = 0, bf = 0;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, k_theta32<M>, kTileThreads, R::THETA_SMEM)) ||
+      (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf, k_force32<M>, kTileThreads, R::FORCE_SMEM))) {
+    *out = e;
+    return;
+  }
+  bt = std::max(bt, 1);
+  bf = std::max(bf, 1);
+  gr.grid_theta = std::min(gr.n_tiles, bt * n_sm);
+  gr.grid_force = std::min(gr.n_tiles, bf * n_sm);
+}
+
+cudaError_t dense32_prepare_group(DenseGroup &gr, int n_sm) {
+  cudaError_t e = cudaErrorInvalidValue;
+  LPS_DISPATCH_M(gr.m, prepare32_m, gr, n_sm, &e);
+  return e;
+}
+
+template <int M>
+static void theta32_m(const DenseGroup &gr, const LaunchGeo &lg, const DenseGeo &dg, const StepPtrs &p,
+                      int ring_u, bool skip_abc, cudaStream_t st) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(gr.grid_theta);
+  cfg.blockDim = dim3(kTileThreads);
+  cfg.dynamicSmemBytes = Region32<M>::THETA_SMEM;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributePriority;
+  attr[0].val.priority = dg.tile_priority;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, k_theta32<M>, gr.maps.u32[ring_u & 1], gr.maps.type, lg.geo, dg.tiles, gr.tile_begin,
+                     gr.n_tiles, p, dg.pitch, skip_abc ? 1 : 0, gr.sched, dg.d_err);
+}
+
+template <int M>
+static void force32_m(const DenseGroup &gr, const LaunchGeo &lg, const DenseGeo &dg, const StepPtrs &p,
+                      int ring_u, int ring_th, bool abc_on, bool first, int *d_step, cudaStream_t st) {
+  k_force32<M><<<gr.grid_force, kTileThreads, Region32<M>::FORCE_SMEM, st>>>(
+      gr.maps.u32[ring_u & 1], gr.maps.th[ring_th], gr.maps.coef32, gr.maps.type, lg.geo, dg.tiles, gr.tile_begin,
+      gr.n_tiles, p, dg.pitch, abc_on ? 1 : 0, first ? 1 : 0, d_step, gr.sched + 2, dg.d_err);
+}
+
+void launch_theta32_group(const DenseGroup &gr, const LaunchGeo &lg, const DenseGeo &dg, const StepPtrs &p,
+                          int ring_u, bool skip_abc, cudaStream_t st) {
+  LPS_DISPATCH_M(gr.m, theta32_m, gr, lg, dg, p, ring_u, skip_abc, st);
+}
+
+void launch_force32_group(const DenseGroup &gr, const LaunchGeo &lg, const DenseGeo &dg, const StepPtrs &p,
+                          int ring_u, int ring_th, bool abc_on, bool first, int *d_step, cudaStream_t st) {
+  LPS_DISPATCH_M(gr.m, force32_m, gr, lg, dg, p, ring_u, ring_th, abc_on, first, d_step, st);
+}
+
+}  // namespace lps
