@@ -243,16 +243,12 @@ void fill_params(InstParams &P, const lps_problem &p, const lps_options &o, cons
 int upload_abc(lps_handle *h, const HostAbc &H, int total_abc, const std::vector<int> &abc_of) {
   Abc &B = h->lg.abc;
   int s;
-  int *a_node, *a_inst, *a_cl_off, *a_cl_len, *a_cl_idx, *a_idw_off, *a_idw_len, *a_idw_idx, *a_cl_src;
+  int *a_node, *a_inst, *a_cl_off, *a_cl_len, *a_cl_idx, *a_idw_off, *a_idw_len, *a_idw_idx;
   uint8_t *a_writes, *a_active;
   double *a_gu, *a_gv, *a_idw_w;
   double *a_gth;
   // which cloud entries are themselves G_u-written nodes (their u^n lives in
   // the previous step's G_u result until the next predictor merges it)
-  std::vector<int> cl_src(H.cl_idx.size());
-  for (size_t e = 0; e < H.cl_idx.size(); e++) cl_src[e] = abc_of[H.cl_idx[e]];
-  if ((s = dev_upload(h, &a_cl_src, cl_src))) return s;
-  B.cl_src = a_cl_src;
   if ((s = dev_upload(h, &a_node, H.node)) || (s = dev_upload(h, &a_inst, H.inst)) ||
       (s = dev_upload(h, &a_cl_off, H.cl_off)) || (s = dev_upload(h, &a_cl_len, H.cl_len)) ||
       (s = dev_upload(h, &a_cl_idx, H.cl_idx)) || (s = dev_upload(h, &a_idw_off, H.idw_off)) ||
@@ -541,7 +537,7 @@ int build_dense(lps_handle *h, const lps_problem *probs, const std::vector<Latti
       for (int q0 = 0; q0 < cols[k]; q0 += kTileCols) {
         const int region_row = row_begin[k] + r0, region_col = q0;
         const long first = (long)(region_row + M) * P + region_col + M;
-        bool any = false, full = true, abc = false;
+        bool any = false, full = true;
         for (int r = 0; r < kTileRows; r++)
           for (int q = 0; q < kTileCols; q++) {
             const long c = first + (long)r * P + q;
@@ -550,14 +546,8 @@ int build_dense(lps_handle *h, const lps_problem *probs, const std::vector<Latti
             for (size_t j = 0; j < A.size() && full; j++)
               if (!(type[c + (long)A[j] * P + B[j]] & kExists)) full = false;
           }
-        for (int r = 0; r < kTileRows + 2 * M && !abc; r++)
-          for (int q = 0; q < kTileCols + 2 * M; q++)
-            if (type[(long)(region_row + r) * P + region_col + q] & kActiveAbc) {
-              abc = true;
-              break;
-            }
         if (any)
-          tiles.push_back(DenseTile{region_row, region_col, k, (full ? kTileFull : 0) | (abc ? kTileAbc : 0)});
+          tiles.push_back(DenseTile{region_row, region_col, k, full ? kTileFull : 0});
       }
   }
   std::stable_sort(tiles.begin(), tiles.end(), [&](const DenseTile &x, const DenseTile &y) {
@@ -705,7 +695,8 @@ int enqueue_step(lps_handle *h, int64_t n, bool diag, const Mark *mark = nullptr
     k++;
   }
   if (diag) {
-    const bool abc = h->opt.abcs_step != -1 && h->lg.abc.n_abc > 0;
+    // the dense step merges G_u results into the ring itself (k_abc_predict)
+    const bool abc = h->opt.abcs_step != -1 && h->lg.abc.n_abc > 0 && h->path != LPS_PATH_DENSE;
     if (abc) {
       launch_merge_abc(h->lg, p.u_np1, p.s_abc, st);
       M("merge_abc");

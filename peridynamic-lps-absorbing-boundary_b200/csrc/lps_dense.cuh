@@ -35,7 +35,6 @@ constexpr int kUring = 4;       // displacement ring depth of the dense path
 
 // tile flags
 constexpr int kTileFull = 1;    // every neighbour of every owned node exists
-constexpr int kTileAbc = 2;     // the staged region holds an active ABC node
 
 struct DenseTile {
   int row;    // global row of the staged region's first row

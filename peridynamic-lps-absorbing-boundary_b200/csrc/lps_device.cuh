@@ -98,7 +98,6 @@ struct Abc {
   const uint8_t *active;       // BCTypes[2 node] == 1
   const int *cl_off, *cl_len;  // compacted cloud list (k != -1 only)
   const int *cl_idx;           // global node index per cloud entry
-  const int *cl_src;           // per cloud entry: ABC entry whose G_u writes that node, or -1
   const double *gu;            // per entry 8 doubles: row x [4], row y [4]
   const double *gv;            // same
   const double *gth;           // per node: rows theta^n, theta^{n-1} of cl_len weights

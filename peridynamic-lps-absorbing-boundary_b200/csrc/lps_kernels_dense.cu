@@ -222,35 +222,13 @@ __global__ void __launch_bounds__(kTileThreads, 2)
       if (nx < n_tiles) issue(stage ^ 1, nx);
     }
     const DenseTile t = tiles[tile_begin + tile];
-    const InstParams &P = c_inst[t.inst];
-    double2 *su = reinterpret_cast<double2 *>(smem + stage * R::THETA_STAGE);
-    uint8_t *sty = reinterpret_cast<uint8_t *>(smem + stage * R::THETA_STAGE + R::T_TY);
+    const double2 *su = reinterpret_cast<const double2 *>(smem + stage * R::THETA_STAGE);
+    const uint8_t *sty = reinterpret_cast<const uint8_t *>(smem + stage * R::THETA_STAGE + R::T_TY);
     const int r0 = 2 * warp;
     // m_i of the owned cells, fetched while the copy lands
     const size_t cell0 = (size_t)(t.row + M + r0) * pitch + t.col + M + lane;
     const double mi0 = g.m[cell0], mi1 = g.m[cell0 + pitch];
     if (!mbar_wait_bounded(&bar[stage], (it >> 1) & 1, err)) return;
-    if (t.flags & kTileAbc) {
-      // ABC nodes: u^n from the last G_u, predicted here (src/main.cpp:727)
-      for (int q = tid; q < R::CELLS; q += kTileThreads) {
-        const int rr = q / R::RC, cc = q - rr * R::RC;
-        if (!(sty[rr * R::RT + cc] & kActiveAbc)) continue;
-        const size_t cell = (size_t)(t.row + rr) * pitch + t.col + cc;
-        const double2 u = p.s_prev[g.abc_of[cell]], v = p.v_n[cell], a = p.a_n[cell];
-        double2 vh, up;
-        vh.x = v.x + P.half_dt * a.x;
-        vh.y = v.y + P.half_dt * a.y;
-        up.x = u.x + P.dt * vh.x;
-        up.y = u.y + P.dt * vh.y;
-        su[q] = up;
-        if (rr >= M && rr < M + kTileRows && cc >= M && cc < M + kTileCols) {
-          p.u_np1[cell] = up;
-          p.vh[cell] = vh;
-          p.u_n[cell] = u;
-        }
-      }
-      __syncthreads();
-    }
     double th[2];
     if (t.flags & kTileFull)
       theta_tile<M, true>(su, sty, r0, lane, th);
@@ -379,11 +357,31 @@ __global__ void __launch_bounds__(256) k_abc_uv(Abc ab, StepPtrs p) {
   abc_uv_warp(ab, a, p);
 }
 
+// End of a dense step at the absorbing boundary, after the force tiles and
+// G_u/G_v: this step's G_u result u^{n+1} goes into the displacement ring,
+// and u^{n+2} is predicted there from it, the G_v velocity and the new
+// acceleration (src/main.cpp:725-728), so the next step's tiles stage every
+// cell straight from the rings.
+__global__ void __launch_bounds__(256) k_abc_predict(Abc ab, StepPtrs p) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= ab.n_abc || !ab.writes[a]) return;
+  const int node = ab.node[a];
+  const InstParams &P = c_inst[ab.inst[a]];
+  const double2 u = p.s_abc[a], v = p.v_np1[node], acc = p.a_np1[node];
+  double2 vh, up;
+  vh.x = v.x + P.half_dt * acc.x;
+  vh.y = v.y + P.half_dt * acc.y;
+  up.x = u.x + P.dt * vh.x;
+  up.y = u.y + P.dt * vh.y;
+  p.u_np1[node] = u;
+  p.u_np2[node] = up;
+  p.vh[node] = vh;
+  if (p.u32_np2) p.u32_np2[node] = make_float2((float)up.x, (float)up.y);
+}
+
 // G_u (src/main.cpp:883-916) and G_v (:933-974) of one step for one ABC node
-// per warp, for the dense path.  It runs while the dilatation tiles of the
-// same step are predicting and merging displacements, so u^n of a cloud node
-// that is itself G_u-written comes from the previous step's G_u result
-// (p.s_prev), and the result goes to the other buffer (p.s_abc).
+// per warp, for the dense path.  u^n at ABC nodes is already in the ring (the
+// previous step's k_abc_predict merged it); the result goes to p.s_abc.
 __global__ void __launch_bounds__(256) k_abc_uv_dense(Abc ab, StepPtrs p) {
   const int lane = threadIdx.x & 31;
   const int a = blockIdx.x * kAbcWarpsPerBlock + (threadIdx.x >> 5);
@@ -399,9 +397,8 @@ __global__ void __launch_bounds__(256) k_abc_uv_dense(Abc ab, StepPtrs p) {
     const int ea = e0 + lane, eb = e0 + 32 + lane;
     const bool va = ea < len, vb = eb < len;
     const int ka = va ? __ldg(ab.cl_idx + off + ea) : 0, kb = vb ? __ldg(ab.cl_idx + off + eb) : 0;
-    const int sa = va ? __ldg(ab.cl_src + off + ea) : -1, sb = vb ? __ldg(ab.cl_src + off + eb) : -1;
-    const double2 una = va ? (sa >= 0 ? p.s_prev[sa] : p.u_n[ka]) : z, uma = va ? p.u_nm1[ka] : z;
-    const double2 unb = vb ? (sb >= 0 ? p.s_prev[sb] : p.u_n[kb]) : z, umb = vb ? p.u_nm1[kb] : z;
+    const double2 una = va ? p.u_n[ka] : z, uma = va ? p.u_nm1[ka] : z;
+    const double2 unb = vb ? p.u_n[kb] : z, umb = vb ? p.u_nm1[kb] : z;
     if (va) g_entry(gu, len, ea, una, uma, ux, uy);
     if (vb) g_entry(gu, len, eb, unb, umb, ux, uy);
     if (!kin) {
@@ -422,7 +419,7 @@ __global__ void __launch_bounds__(256) k_abc_uv_dense(Abc ab, StepPtrs p) {
     p.s_abc[a] = make_double2(ux, uy);
     if (kin) {
       // v = (u^{n+1} - u^n) / dt with this node's u^n, src/main.cpp:940-943
-      const double2 un = p.s_prev[a];
+      const double2 un = p.u_n[node];
       p.v_np1[node] = make_double2((ux - un.x) / P.dt, (uy - un.y) / P.dt);
     } else {
       p.v_np1[node] = make_double2(vx, vy);
@@ -562,6 +559,11 @@ static cudaError_t prepare_m(DenseGroup &gr, int n_sm) {
     return e;
   if ((e = cudaFuncSetAttribute(k_force_tma<M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 Region<M>::FORCE_SMEM)))
+    return e;
+  if ((e = cudaFuncSetAttribute(k_theta_tma<M>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                cudaSharedmemCarveoutMaxShared)) ||
+      (e = cudaFuncSetAttribute(k_force_tma<M>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                cudaSharedmemCarveoutMaxShared)))
     return e;
   int bt = 0, bf = 0;
   if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, k_theta_tma<M>, kTileThreads, Region<M>::THETA_SMEM)))
@@ -741,7 +743,12 @@ int enqueue_dense_step(const DenseGeo &dg, const LaunchGeo &lg, const StepPtrs &
     first = false;
     k++;
   }
-  if (abc && fork) cudaStreamWaitEvent(st, dg.ev_join[1], 0);
+  if (abc) {
+    if (fork) cudaStreamWaitEvent(st, dg.ev_join[1], 0);
+    k_abc_predict<<<(lg.abc.n_abc + 255) / 256, 256, 0, st>>>(lg.abc, p);
+    if (mark) (*mark)("abc_predict");
+    k++;
+  }
   if (mark) (*mark)("force_tiles");
   return k;
 }

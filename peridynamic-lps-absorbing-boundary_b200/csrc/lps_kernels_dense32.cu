@@ -195,35 +195,12 @@ __global__ void __launch_bounds__(kTileThreads, 2)
     }
     const DenseTile t = tiles[tile_begin + tile];
     const InstParams &P = c_inst[t.inst];
-    float2 *su = reinterpret_cast<float2 *>(smem + stage * R::THETA_STAGE);
-    uint8_t *sty = reinterpret_cast<uint8_t *>(smem + stage * R::THETA_STAGE + R::T_TY);
+    const float2 *su = reinterpret_cast<const float2 *>(smem + stage * R::THETA_STAGE);
+    const uint8_t *sty = reinterpret_cast<const uint8_t *>(smem + stage * R::THETA_STAGE + R::T_TY);
     const int r0 = 2 * warp;
     const size_t cell0 = (size_t)(t.row + M + r0) * pitch + t.col + M + lane;
     const double mi0 = g.m[cell0], mi1 = g.m[cell0 + pitch];
     if (!mbar_wait_bounded(&bar[stage], (it >> 1) & 1, err)) return;
-    if (t.flags & kTileAbc) {
-      // ABC nodes: u^n from the last G_u, predicted here in FP64 (src/main.cpp:727)
-      for (int q = tid; q < R::CELLS; q += kTileThreads) {
-        const int rr = q / R::RC, cc = q - rr * R::RC;
-        if (!(sty[rr * R::RT + cc] & kActiveAbc)) continue;
-        const size_t cell = (size_t)(t.row + rr) * pitch + t.col + cc;
-        const double2 u = p.s_prev[g.abc_of[cell]], v = p.v_n[cell], a = p.a_n[cell];
-        double2 vh, up;
-        vh.x = v.x + P.half_dt * a.x;
-        vh.y = v.y + P.half_dt * a.y;
-        up.x = u.x + P.dt * vh.x;
-        up.y = u.y + P.dt * vh.y;
-        const float2 up32 = make_float2((float)up.x, (float)up.y);
-        su[q] = up32;
-        if (rr >= M && rr < M + kTileRows && cc >= M && cc < M + kTileCols) {
-          p.u_np1[cell] = up;
-          p.u32_np1[cell] = up32;
-          p.vh[cell] = vh;
-          p.u_n[cell] = u;
-        }
-      }
-      __syncthreads();
-    }
     float th[2];
     if (t.flags & kTileFull)
       theta_tile32<M, true>(su, sty, r0, lane, th);
@@ -249,7 +226,7 @@ __global__ void __launch_bounds__(kTileThreads, 2)
 // After the copy lands, (theta, coef) become (A', B) = (dx 2(l-m)/m theta,
 // 8 mu/m) in the coef slot; absent neighbours and m <= 0 get A' = B = 0.
 template <int M>
-__global__ void __launch_bounds__(kTileThreads, 2)
+__global__ void __launch_bounds__(kTileThreads, 3)
     k_force32(const __grid_constant__ CUtensorMap map_u, const __grid_constant__ CUtensorMap map_th,
               const __grid_constant__ CUtensorMap map_coef, const __grid_constant__ CUtensorMap map_type, Geo g,
               const DenseTile *__restrict__ tiles, int tile_begin, int n_tiles, StepPtrs p, int pitch, int abc_on,
@@ -295,7 +272,9 @@ __global__ void __launch_bounds__(kTileThreads, 2)
     const uint8_t *sty = reinterpret_cast<const uint8_t *>(base + R::F_TY);
     const int r0 = 2 * warp;
     const size_t cell0 = (size_t)(t.row + M + r0) * pitch + t.col + M + lane;
+    // corrector / predictor inputs of the owned cells, fetched while the copy lands
     const double2 vh0 = p.vh[cell0], vh1 = p.vh[cell0 + pitch];
+    const double2 un0 = p.u_np1[cell0], un1 = p.u_np1[cell0 + pitch];
     if (!mbar_wait_bounded(&bar[stage], (it >> 1) & 1, err)) return;
     const float dxf = (float)P.dx;
     for (int q = tid; q < R::CELLS; q += kTileThreads) {
@@ -328,7 +307,7 @@ __global__ void __launch_bounds__(kTileThreads, 2)
       v.y = vh.y + P.half_dt * acc.y;
       vh2.x = v.x + P.half_dt * acc.x;
       vh2.y = v.y + P.half_dt * acc.y;
-      const double2 u = p.u_np1[cell];
+      const double2 u = k == 0 ? un0 : un1;
       un.x = u.x + P.dt * vh2.x;
       un.y = u.y + P.dt * vh2.y;
       p.v_np1[cell] = v;
@@ -350,7 +329,11 @@ static void prepare32_m(DenseGroup &gr, int n_sm, cudaError_t *out) {
   cudaError_t e;
   *out = cudaSuccess;
   if ((e = cudaFuncSetAttribute(k_theta32<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, R::THETA_SMEM)) ||
-      (e = cudaFuncSetAttribute(k_force32<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, R::FORCE_SMEM))) {
+      (e = cudaFuncSetAttribute(k_force32<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, R::FORCE_SMEM)) ||
+      (e = cudaFuncSetAttribute(k_theta32<M>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                cudaSharedmemCarveoutMaxShared)) ||
+      (e = cudaFuncSetAttribute(k_force32<M>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                cudaSharedmemCarveoutMaxShared))) {
     *out = e;
     return;
   }
