@@ -51,7 +51,9 @@ def parse():
     ap.add_argument("--workload", choices=["poisson7", "example1"], default="poisson7")
     ap.add_argument("--time-steps", type=int, default=4000)
     ap.add_argument("--diag-every", type=int, default=30)
-    ap.add_argument("--precision", default="fp64")
+    ap.add_argument("--precision", choices=["both", "fp64", "fp32_mixed"], default="both",
+                    help="both: the FP32-mixed form is the headline value, the FP64 plain form "
+                         "is timed beside it on the same workload")
     ap.add_argument("--path", default="auto")
     ap.add_argument("--cpu-sample-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -70,7 +72,8 @@ def workload_config(name, sets, args):
             "instances": len(sets), "nodes_per_instance": sets[0].n_nodes,
             "abc_nodes_per_instance": sets[0].n_abc, "cloud_size": sets[0].max_cloud,
             "neighbours": 68, "time_steps_per_run": args.time_steps, "diag_every": args.diag_every,
-            "precision": args.precision, "path": args.path,
+            "precision": ("fp32_mixed (value), fp64 (beside it)" if args.precision == "both"
+                          else args.precision), "path": args.path,
             "l2": "flushed (256 MiB write) before each timed run; working set > L2"}
 
 
@@ -186,20 +189,25 @@ def measured_peak_hbm():
     return 6650.0, "fallback"
 
 
-def algorithmic_bytes(sets, kernel):
-    """Compulsory DRAM bytes of one launch of `kernel` in this build's FP64
-    layout (each array read or written once per launch).  Returns
-    (bytes, grading_bytes): the second is the per-node figure the roofline is
-    graded against (force pass 80 B/node, step 168 B/node + 148 C B per ABC
-    node), or None where that figure does not apply."""
+def algorithmic_bytes(sets, kernel, precision="fp64"):
+    """Compulsory DRAM bytes of one launch of `kernel` in this build's layout
+    (each array read or written once per launch).  Returns (bytes,
+    grading_bytes): the second is the per-node figure the roofline is graded
+    against (force pass 80 B/node FP64, 56 B/node FP32-mixed; step 168 B/node
+    FP64, 140 B/node FP32-mixed; + 148 C B per ABC node), or None where that
+    figure does not apply."""
     n = sum(s.n_nodes for s in sets)
     abc = sum(s.n_abc * s.max_cloud for s in sets)
+    f32 = precision == "fp32_mixed"
+    step_node = 140 if f32 else 168
     table = {
-        # force + corrector + next predictor: read u_pred 16, theta 8, 8mu/m 8,
-        # vh 16; write a 16, v 16, vh 16, u_pred(next) 16
-        "force_tiles": (112 * n, 80 * n),
-        # dilatation: read u_pred 16, m 8; write theta 8
-        "theta_tiles": (32 * n, None),
+        # FP64: read u_pred 16, theta 8, coef 16, vh 16; write a 16, v 16,
+        # vh 16, u_pred(next) 16.  FP32-mixed: read u_pred32 8, theta 8,
+        # coef32 8, vh 16, u_pred 16; write a 16, v 16, vh 16, u_pred(next) 16,
+        # u_pred32(next) 8
+        "force_tiles": ((128 if f32 else 120) * n, (56 if f32 else 80) * n),
+        # dilatation: read u_pred 16 (FP32-mixed: 8), m 8; write theta 8
+        "theta_tiles": ((24 if f32 else 32) * n, None),
         # G_u, G_v: 2 x 8C doubles + 4C index bytes per ABC node
         "abc_uv": (132 * abc, None),
         # G_theta: 2C doubles + 4C index bytes per ABC node
@@ -208,7 +216,10 @@ def algorithmic_bytes(sets, kernel):
         "predict_csr": (80 * n, None),
         "theta_csr": (32 * n, None),
         "force_csr": (80 * n + 132 * abc, 80 * n),
-        "step": (168 * n + 148 * abc, 168 * n + 148 * abc),
+        # end-of-step ABC merge + prediction: read s 16, v 16, a 16; write
+        # u 16, u_pred 16, vh 16 (+ u_pred32 8) per ABC node
+        "abc_predict": (sum(s.n_abc for s in sets) * (104 if f32 else 96), None),
+        "step": (step_node * n + 148 * abc, step_node * n + 148 * abc),
     }
     return table.get(kernel, (None, None))
 
@@ -223,7 +234,7 @@ def measured_traffic(kernel):
 
 
 # ---------------------------------------------------------------------------
-def run_ours(args, rank, world, local_rank):
+def run_ours(args, rank, world, local_rank, precision, with_cpu=True):
     import numpy as np
     import torch
     import torch.distributed as dist
@@ -233,7 +244,7 @@ def run_ours(args, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
     sets = workload_sets(args.workload, args.time_steps)
     stream = torch.cuda.Stream(device=dev)
-    sv = Solver(sets, precision=args.precision, path=args.path, device=local_rank,
+    sv = Solver(sets, precision=precision, path=args.path, device=local_rank,
                 stream=stream.cuda_stream)
     info = sv.info(0)
     T, K, W = args.time_steps, args.steps, args.warmup
@@ -269,10 +280,11 @@ def run_ours(args, rank, world, local_rank):
     launches = sv.kernel_launches - launches0
     clk = clocks.stop()
     ms = sum(a.elapsed_time(b) for a, b in ev)
-    final_dE = []
+    final_dE, final_u = [], []
     for k in range(len(sets)):
         d = sv.read_diag(k)
         final_dE.append(float(d["dE_rel"][-1]) if len(d) else None)
+        final_u.append(sv.download(k)["u"])
     t = torch.tensor([ms], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -311,17 +323,17 @@ def run_ours(args, rank, world, local_rank):
     top = max(prof.items(), key=lambda kv: kv[1][1])
     name, (nl, tot) = top
     per_launch_ms = tot / nl
-    ab, ab_grade = algorithmic_bytes(sets, name)
+    ab, ab_grade = algorithmic_bytes(sets, name, precision)
     peak, peak_kind = measured_peak_hbm()
     gbs = lambda b, ms: b / (ms / 1e3) / 1e9 if b else None  # noqa: E731
     achieved = gbs(ab_grade if ab_grade else ab, per_launch_ms)
     step_ms = sum(v[1] for v in prof.values()) / 120.0
     kernels = {}
     for k, v in prof.items():
-        b, _ = algorithmic_bytes(sets, k)
+        b, _ = algorithmic_bytes(sets, k, precision)
         kernels[k] = {"launches": v[0], "ms_per_launch": v[1] / v[0], "algorithmic_bytes": b,
                       "achieved_gbs": gbs(b, v[1] / v[0]), "traffic": measured_traffic(k)}
-    step_bytes, _ = algorithmic_bytes(sets, "step")
+    step_bytes, _ = algorithmic_bytes(sets, "step", precision)
     roofline = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
                 "traffic": measured_traffic(name), "algorithmic_bytes_per_launch": ab_grade or ab,
@@ -333,14 +345,14 @@ def run_ours(args, rank, world, local_rank):
 
     out = {"metric": METRIC, "value": value, "unit": "node-steps/s", "n_gpus": world, "steps": K,
            "warmup": W, "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak",
-           "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+           "vs_baseline": None, "dtype": "f64" if precision == "fp64" else "f32+f64",
            "data": "synthetic (generated Example-1 geometry; passive averaging ABC operators)",
            "config": workload_config(args.workload, sets, args) | {"parallelism": f"replicas{world}"},
            "e2e": {"value": e2e_value, "unit": "node-steps/s", "h2d_bytes_per_step": h2d,
                    "d2h_bytes_per_step": d2h},
            "gpu_launches": launches, "roofline": roofline, "clocks": clk,
-           "kernel_path": info["path"], "final_dE_rel": final_dE}
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+           "kernel_path": info["path"], "final_dE_rel": final_dE, "_u": final_u}
+    if with_cpu and rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         s_cpu = [s for s in sets if abs(s.nu - 0.25) < 1e-12][0] if len(sets) > 1 else sets[0]
         v, sec, kind = cpu_leg(s_cpu, args.cpu_sample_steps, threads)
@@ -387,7 +399,24 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local_rank))
-    out = run_ours(args, rank, world, local_rank)
+    if args.precision == "both":
+        out64 = run_ours(args, rank, world, local_rank, "fp64", with_cpu=False)
+        out = run_ours(args, rank, world, local_rank, "fp32_mixed")
+        out["fp64"] = {"value": out64["value"], "ms_per_step": out64["ms_per_step"],
+                       "e2e": out64["e2e"]["value"], "gpu_launches": out64["gpu_launches"],
+                       "final_dE_rel": out64["final_dE_rel"], "clocks": out64["clocks"],
+                       "kernels_ms": {k: v["ms_per_launch"] for k, v in out64["roofline"]["kernels"].items()},
+                       "time_step_ms": out64["roofline"]["time_step_ms"],
+                       "step_hbm_frac": out64["roofline"]["step_hbm_frac"]}
+        out["fp32_mixed_over_fp64"] = out["value"] / out64["value"]
+        import numpy as np
+        rel = [float(np.linalg.norm(a - b) / np.linalg.norm(b)) for a, b in zip(out["_u"], out64["_u"])]
+        dde = [abs(a - b) for a, b in zip(out["final_dE_rel"], out64["final_dE_rel"])]
+        out["fp32_mixed_error_vs_fp64"] = {"u_rel_l2_max": max(rel), "final_dE_rel_absdiff_max": max(dde),
+                                           "u_rel_l2": rel}
+    else:
+        out = run_ours(args, rank, world, local_rank, args.precision)
+    out.pop("_u", None)
     if rank == 0:
         print(json.dumps(out), flush=True)
     if world > 1:

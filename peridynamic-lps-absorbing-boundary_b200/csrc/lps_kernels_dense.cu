@@ -743,13 +743,13 @@ int enqueue_dense_step(const DenseGeo &dg, const LaunchGeo &lg, const StepPtrs &
     first = false;
     k++;
   }
+  if (mark) (*mark)("force_tiles");
   if (abc) {
     if (fork) cudaStreamWaitEvent(st, dg.ev_join[1], 0);
     k_abc_predict<<<(lg.abc.n_abc + 255) / 256, 256, 0, st>>>(lg.abc, p);
     if (mark) (*mark)("abc_predict");
     k++;
   }
-  if (mark) (*mark)("force_tiles");
   return k;
 }
 
