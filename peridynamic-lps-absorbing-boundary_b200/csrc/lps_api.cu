@@ -63,7 +63,6 @@ struct lps_handle {
   double *TH[3] = {};
   double2 *U0 = nullptr, *V0 = nullptr;
   float2 *U32[2] = {};        // FP32-mixed form: FP32 copies of the predicted level, by step parity
-  float2 *L32[2] = {};        // FP32-mixed form: FP32 remainders u - U32
   float2 *coef32 = nullptr;   // FP32-mixed form: (2(l-m)/m_i, 8mu/m_i) as float2
   // diagnostics
   DiagPartial *partials = nullptr;
@@ -613,7 +612,7 @@ int finish_dense(lps_handle *h) {
   const uint8_t *type = h->lg.geo.type;
   for (auto &gr : D.groups) {
     const int s = dense_encode_maps(gr, D.pitch, D.total_rows, h->U, h->TH, coef, type, D.fp32 ? h->U32 : nullptr,
-                                    h->L32, h->coef32, h->err);
+                                    h->coef32, h->err);
     if (s) return s;
   }
   LPS_CUDA_TRY(h, cudaStreamCreateWithFlags(&D.side, cudaStreamNonBlocking));
@@ -656,9 +655,7 @@ StepPtrs step_ptrs(lps_handle *h, int64_t n) {
   p.th_nm1 = h->TH[um];
   p.th_np1 = h->TH[u1];
   p.u32_np1 = h->U32[(n + 1) % 2];
-  p.l32_np1 = h->L32[(n + 1) % 2];
   p.u32_np2 = h->U32[n % 2];
-  p.l32_np2 = h->L32[n % 2];
   if (h->path == LPS_PATH_DENSE) {
     // the dense step computes G_u concurrently with the predictor that still
     // reads the previous result, so the two alternate by step parity
@@ -809,7 +806,7 @@ int do_reset(lps_handle *h) {
   }
   // dense path: the force pass predicts the next level, so level 1 is
   // predicted here (src/main.cpp:727 with a^0 = 0)
-  if (h->path == LPS_PATH_DENSE) launch_dense_reset_predict(h->lg, h->U0, h->V0, h->U[1], h->U32[1], h->L32[1], h->VH, st);
+  if (h->path == LPS_PATH_DENSE) launch_dense_reset_predict(h->lg, h->U0, h->V0, h->U[1], h->U32[1], h->VH, st);
   LPS_CUDA_TRY(h, cudaMemsetAsync(h->d_step, 0, sizeof(int), st));
   LPS_CUDA_TRY(h, cudaMemsetAsync(h->log_count, 0, sizeof(int) * h->n_inst, st));
   LPS_CUDA_TRY(h, cudaGetLastError());
@@ -845,9 +842,8 @@ int alloc_state(lps_handle *h) {
   LPS_CUDA_TRY(h, cudaMemset(h->VH, 0, sizeof(double2) * n));
   if (h->dg.fp32)
     for (int r = 0; r < 2; r++) {
-      if ((s = dev_alloc(h, &h->U32[r], n)) || (s = dev_alloc(h, &h->L32[r], n))) return s;
+      if ((s = dev_alloc(h, &h->U32[r], n))) return s;
       LPS_CUDA_TRY(h, cudaMemset(h->U32[r], 0, sizeof(float2) * n));
-      LPS_CUDA_TRY(h, cudaMemset(h->L32[r], 0, sizeof(float2) * n));
     }
   const int n_part = h->lg.n_node_blocks + (h->n_abc_total + kNodeBlock - 1) / kNodeBlock + 1;
   h->log_capacity = 1024;

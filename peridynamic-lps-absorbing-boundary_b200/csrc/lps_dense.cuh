@@ -50,7 +50,6 @@ struct DenseMaps {
   CUtensorMap coef;       // (2(l-m)/m_i, 8 mu/m_i)
   CUtensorMap type;       // u8 node type
   CUtensorMap u32[2];     // FP32-mixed form: FP32 predicted displacements, by step parity
-  CUtensorMap l32[2];     // FP32-mixed form: their FP32 remainders
   CUtensorMap coef32;     // FP32-mixed form: coef as float2
 };
 
@@ -94,8 +93,8 @@ cudaError_t upload_dense_constants(int m, double dx, double dy, double delta, cu
 // Encodes the TMA descriptors of group g over the given buffers (U32 and
 // coef32 only in the FP32-mixed form, else null).
 int dense_encode_maps(DenseGroup &g, int pitch, int total_rows, double2 *const *U, double *const *TH,
-                      const double2 *coef, const uint8_t *type, float2 *const *U32, float2 *const *L32,
-                      const float2 *coef32, std::string &err);
+                      const double2 *coef, const uint8_t *type, float2 *const *U32, const float2 *coef32,
+                      std::string &err);
 // Sets shared-memory limits and the persistent grid sizes of each group.
 cudaError_t dense_prepare(DenseGeo &dg);
 
@@ -110,10 +109,10 @@ void launch_force32_group(const DenseGroup &gr, const LaunchGeo &lg, const Dense
 // beside both tile passes.
 int enqueue_dense_step(const DenseGeo &dg, const LaunchGeo &lg, const StepPtrs &p, int *d_step,
                        cudaStream_t st, const Mark *mark, int ring_u);
-// Reset helpers: predicted u^1 (and its FP32 pair u32_1 / l32_1 when not
-// null) and vh for every cell from u^0, v^0.
+// Reset helpers: predicted u^1 (and its FP32 copy u32_1 when not null) and
+// vh for every cell from u^0, v^0.
 void launch_dense_reset_predict(const LaunchGeo &lg, const double2 *u0, const double2 *v0, double2 *u1,
-                                float2 *u32_1, float2 *l32_1, double2 *vh, cudaStream_t st);
+                                float2 *u32_1, double2 *vh, cudaStream_t st);
 void launch_theta_dense_init(const DenseGeo &dg, const LaunchGeo &lg, const double2 *u, double *theta,
                              cudaStream_t st);
 void launch_diag_dense(const DenseGeo &dg, const LaunchGeo &lg, const double2 *u, const double2 *v,

@@ -54,15 +54,6 @@ struct InstParams {
   int pad0;
 };
 
-// u rounded to FP32 (hi) and the FP32 rounding of the remainder (lo): hi + lo
-// carries u to about 2^-48 relative, so differences of neighbouring
-// displacements keep their digits in FP32 arithmetic.
-__device__ __forceinline__ void split_store(float2 *hi, float2 *lo, size_t i, double2 u) {
-  const float2 h = make_float2((float)u.x, (float)u.y);
-  hi[i] = h;
-  lo[i] = make_float2((float)(u.x - (double)h.x), (float)(u.y - (double)h.y));
-}
-
 // Buffer pointers of one time step, resolved on the host from the ring phase.
 struct StepPtrs {
   double2 *u_n;            // u^n (ABC entries merged in by the predictor)
@@ -78,10 +69,8 @@ struct StepPtrs {
   double2 *s_abc;          // G_u result u^{n+1} at ABC nodes, merged next step
   double2 *u_np2;          // dense path: predicted u^{n+2}, written by the force pass
   const double2 *s_prev;   // dense path: G_u result of the previous step (u^n at ABC nodes)
-  float2 *u32_np1;         // FP32-mixed form: predicted u^{n+1} rounded to FP32 ...
-  float2 *l32_np1;         // ... and the FP32 rounding of its remainder u - u32
-  float2 *u32_np2;         // FP32-mixed form: the same pair for u^{n+2}, written by the
-  float2 *l32_np2;         // force pass
+  float2 *u32_np1;         // FP32-mixed form: FP32 copy of the predicted u^{n+1}
+  float2 *u32_np2;         // FP32-mixed form: FP32 copy of u^{n+2}, written by the force pass
   int th_ring;             // ring index of th_np1
   int pad;
 };

@@ -376,7 +376,7 @@ __global__ void __launch_bounds__(256) k_abc_predict(Abc ab, StepPtrs p) {
   p.u_np1[node] = u;
   p.u_np2[node] = up;
   p.vh[node] = vh;
-  if (p.u32_np2) split_store(p.u32_np2, p.l32_np2, node, up);
+  if (p.u32_np2) p.u32_np2[node] = make_float2((float)up.x, (float)up.y);
 }
 
 // G_u (src/main.cpp:883-916) and G_v (:933-974) of one step for one ABC node
@@ -528,13 +528,12 @@ __global__ void __launch_bounds__(kNodeBlock)
 
 // u^1 = u^0 + dt (v^0 + dt/2 a^0) with a^0 = 0, and vh = v^0, src/main.cpp:727.
 __global__ void __launch_bounds__(256) k_dense_reset_predict(Geo g, const double2 *u0, const double2 *v0,
-                                                              double2 *u1, float2 *u32_1, float2 *l32_1,
-                                                              double2 *vh) {
+                                                              double2 *u1, float2 *u32_1, double2 *vh) {
   const size_t cell = (size_t)blockIdx.x * 256 + threadIdx.x;
   if (cell >= (size_t)g.n_total) return;
   if (!(g.type[cell] & kExists)) {
     u1[cell] = make_double2(0.0, 0.0);
-    if (u32_1) split_store(u32_1, l32_1, cell, make_double2(0.0, 0.0));
+    if (u32_1) u32_1[cell] = make_float2(0.f, 0.f);
     vh[cell] = make_double2(0.0, 0.0);
     return;
   }
@@ -546,7 +545,7 @@ __global__ void __launch_bounds__(256) k_dense_reset_predict(Geo g, const double
   up.x = u.x + P.dt * h.x;
   up.y = u.y + P.dt * h.y;
   u1[cell] = up;
-  if (u32_1) split_store(u32_1, l32_1, cell, up);
+  if (u32_1) u32_1[cell] = make_float2((float)up.x, (float)up.y);
   vh[cell] = h;
 }
 
@@ -630,16 +629,13 @@ bool encode(CUtensorMap *map, CUtensorMapDataType dt, size_t elem, const void *b
 
 template <int M>
 void encode_m(DenseGroup &g, int pitch, int rows, double2 *const *U, double *const *TH, const double2 *coef,
-              const uint8_t *type, float2 *const *U32, float2 *const *L32, const float2 *coef32, bool *ok) {
+              const uint8_t *type, float2 *const *U32, const float2 *coef32, bool *ok) {
   using R = Region<M>;
   bool good = true;
   if (U32) {
-    for (int r = 0; r < 2; r++) {
+    for (int r = 0; r < 2; r++)
       good &= encode(&g.maps.u32[r], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, U32[r], 2ull * pitch, rows, 2 * R::RC,
                      R::RR);
-      good &= encode(&g.maps.l32[r], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, L32[r], 2ull * pitch, rows, 2 * R::RC,
-                     R::RR);
-    }
     good &= encode(&g.maps.coef32, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, coef32, 2ull * pitch, rows, 2 * R::RC,
                    R::RR);
   }
@@ -654,10 +650,10 @@ void encode_m(DenseGroup &g, int pitch, int rows, double2 *const *U, double *con
 }  // namespace
 
 int dense_encode_maps(DenseGroup &g, int pitch, int total_rows, double2 *const *U, double *const *TH,
-                      const double2 *coef, const uint8_t *type, float2 *const *U32, float2 *const *L32,
-                      const float2 *coef32, std::string &err) {
+                      const double2 *coef, const uint8_t *type, float2 *const *U32, const float2 *coef32,
+                      std::string &err) {
   bool ok = false;
-  LPS_DISPATCH_M(g.m, encode_m, g, pitch, total_rows, U, TH, coef, type, U32, L32, coef32, &ok);
+  LPS_DISPATCH_M(g.m, encode_m, g, pitch, total_rows, U, TH, coef, type, U32, coef32, &ok);
   if (!ok) {
     err = "cuTensorMapEncodeTiled failed for the dense layout";
     return LPS_ERR_CUDA;
@@ -758,8 +754,8 @@ int enqueue_dense_step(const DenseGeo &dg, const LaunchGeo &lg, const StepPtrs &
 }
 
 void launch_dense_reset_predict(const LaunchGeo &lg, const double2 *u0, const double2 *v0, double2 *u1,
-                                float2 *u32_1, float2 *l32_1, double2 *vh, cudaStream_t st) {
-  k_dense_reset_predict<<<lg.n_node_blocks, 256, 0, st>>>(lg.geo, u0, v0, u1, u32_1, l32_1, vh);
+                                float2 *u32_1, double2 *vh, cudaStream_t st) {
+  k_dense_reset_predict<<<lg.n_node_blocks, 256, 0, st>>>(lg.geo, u0, v0, u1, u32_1, vh);
 }
 
 void launch_theta_dense_init(const DenseGeo &, const LaunchGeo &lg, const double2 *u, double *theta,

@@ -2,8 +2,8 @@
 //
 // Same two persistent passes as the FP64 form (lps_kernels_dense.cu), with
 // the bond arithmetic in FP32:
-//   k_theta32<M>   dilatation (src/main.cpp:736-761) from the predicted
-//                  displacements split into FP32 hi + lo parts
+//   k_theta32<M>   dilatation (src/main.cpp:736-761) from an FP32 copy of the
+//                  predicted displacements
 //   k_force32<M>   force (:821-874) in FP32; corrector (:922-925) and the next
 //                  predictor (:725-728) in FP64, which also writes the FP32
 //                  copy of the next predicted level
@@ -54,17 +54,6 @@ __host__ __device__ constexpr float sten_q(int Q, int M, int a, int b) {
 template <int M>
 using Region32 = Region<M, 8, 8>;
 
-// Dilatation stage: FP32 displacement (hi) | its FP32 remainder (lo) | type.
-template <int M>
-struct Theta32 {
-  using R = Region32<M>;
-  static constexpr int T_LO = R::align128(R::U_BYTES);
-  static constexpr int T_TY = R::align128(T_LO + R::U_BYTES);
-  static constexpr int STAGE = R::align128(T_TY + R::TY_BYTES);
-  static constexpr int TX = 2 * R::U_BYTES + R::TY_BYTES;
-  static constexpr int SMEM = 2 * STAGE + 64;
-};
-
 // s + x with Kahan's running compensation c (the estimate is s - c).
 __device__ __forceinline__ void kahan_add(float &s, float &c, float x) {
   const float y = x - c;
@@ -73,22 +62,12 @@ __device__ __forceinline__ void kahan_add(float &s, float &c, float x) {
   s = t;
 }
 
-// Thread owns cells (r0, c) and (r0 + 1, c), as in the FP64 form.  The
-// dilatation pair difference u(+) - u(-) is (hi+ - hi-) + (lo+ - lo-): the hi
-// difference is exact for close values and the lo terms restore the digits
-// that rounding u to FP32 dropped.
+// Thread owns cells (r0, c) and (r0 + 1, c), as in the FP64 form.
 template <int M, bool FULL>
-__device__ __forceinline__ void theta_tile32(const float2 *__restrict__ su, const float2 *__restrict__ sl,
-                                             const uint8_t *__restrict__ sty, int r0, int c, float th[2]) {
+__device__ __forceinline__ void theta_tile32(const float2 *__restrict__ su, const uint8_t *__restrict__ sty, int r0,
+                                             int c, float th[2]) {
   using R = Region32<M>;
-  float2 ui[2], li[2];
-  if (!FULL) {
-#pragma unroll
-    for (int k = 0; k < 2; k++) {
-      ui[k] = su[QI<M>(r0 + k, c)];
-      li[k] = sl[QI<M>(r0 + k, c)];
-    }
-  }
+  const float2 ui0 = su[QI<M>(r0, c)], ui1 = su[QI<M>(r0 + 1, c)];
   float S[2] = {0.f, 0.f}, C[2] = {0.f, 0.f}, part[2] = {0.f, 0.f};
   for_each_pair<M>(
       [&](auto ac, auto bc) {
@@ -97,15 +76,15 @@ __device__ __forceinline__ void theta_tile32(const float2 *__restrict__ su, cons
 #pragma unroll
         for (int k = 0; k < 2; k++) {
           const int r = r0 + k;
-          const int qp = QI<M>(r + a, c + b), qm = QI<M>(r - a, c - b);
-          const float2 up = su[qp], um = su[qm], lp = sl[qp], lm = sl[qm];
-          float dx = (up.x - um.x) + (lp.x - lm.x), dy = (up.y - um.y) + (lp.y - lm.y);
+          const float2 up = su[QI<M>(r + a, c + b)], um = su[QI<M>(r - a, c - b)];
+          float dx = up.x - um.x, dy = up.y - um.y;
           if (!FULL) {
             // absent neighbours hold u = 0; restore the -u_i of the present side
             const float mp = (sty[(r + a + M) * R::RT + c + b + M] & kExists) ? 1.f : 0.f;
             const float mm = (sty[(r - a + M) * R::RT + c - b + M] & kExists) ? 1.f : 0.f;
-            dx = fmaf(mm - mp, ui[k].x, fmaf(mm - mp, li[k].x, dx));
-            dy = fmaf(mm - mp, ui[k].y, fmaf(mm - mp, li[k].y, dy));
+            const float2 ui = k == 0 ? ui0 : ui1;
+            dx = fmaf(mm - mp, ui.x, dx);
+            dy = fmaf(mm - mp, ui.y, dy);
           }
           part[k] = fmaf(wx, dx, part[k]);
           part[k] = fmaf(wy, dy, part[k]);
@@ -181,14 +160,13 @@ __device__ __forceinline__ void force_tile32(const float2 *__restrict__ su, cons
 // ---------------------------------------------------------------------------
 // Predicted displacements (FP32 copy) -> dilatation, persistent over tiles.
 template <int M>
-__global__ void __launch_bounds__(kTileThreads, 3)
-    k_theta32(const __grid_constant__ CUtensorMap map_u, const __grid_constant__ CUtensorMap map_l,
-              const __grid_constant__ CUtensorMap map_type, Geo g, const DenseTile *__restrict__ tiles,
-              int tile_begin, int n_tiles, StepPtrs p, int pitch, int skip_abc, int *sched, int *err) {
+__global__ void __launch_bounds__(kTileThreads, 2)
+    k_theta32(const __grid_constant__ CUtensorMap map_u, const __grid_constant__ CUtensorMap map_type, Geo g,
+              const DenseTile *__restrict__ tiles, int tile_begin, int n_tiles, StepPtrs p, int pitch, int skip_abc,
+              int *sched, int *err) {
   using R = Region32<M>;
-  using T = Theta32<M>;
   extern __shared__ __align__(128) unsigned char smem[];
-  uint64_t *bar = reinterpret_cast<uint64_t *>(smem + 2 * T::STAGE);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem + 2 * R::THETA_STAGE);
   int *s_tile = reinterpret_cast<int *>(bar + 2);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (*(volatile int *)err) return;  // an earlier wait timed out: do nothing
@@ -201,11 +179,10 @@ __global__ void __launch_bounds__(kTileThreads, 3)
   __syncthreads();
   auto issue = [&](int stage, int tile) {
     const DenseTile t = tiles[tile_begin + tile];
-    unsigned char *base = smem + stage * T::STAGE;
-    mbar_expect_tx(&bar[stage], T::TX);
+    unsigned char *base = smem + stage * R::THETA_STAGE;
+    mbar_expect_tx(&bar[stage], R::THETA_TX);
     tma_load_2d(base, &map_u, 2 * t.col, t.row, &bar[stage]);
-    tma_load_2d(base + T::T_LO, &map_l, 2 * t.col, t.row, &bar[stage]);
-    tma_load_2d(base + T::T_TY, &map_type, t.col, t.row, &bar[stage]);
+    tma_load_2d(base + R::T_TY, &map_type, t.col, t.row, &bar[stage]);
   };
   int tile = s_tile[0];
   if (tid == 0 && tile < n_tiles) issue(0, tile);
@@ -218,18 +195,17 @@ __global__ void __launch_bounds__(kTileThreads, 3)
     }
     const DenseTile t = tiles[tile_begin + tile];
     const InstParams &P = c_inst[t.inst];
-    const float2 *su = reinterpret_cast<const float2 *>(smem + stage * T::STAGE);
-    const float2 *sl = reinterpret_cast<const float2 *>(smem + stage * T::STAGE + T::T_LO);
-    const uint8_t *sty = reinterpret_cast<const uint8_t *>(smem + stage * T::STAGE + T::T_TY);
+    const float2 *su = reinterpret_cast<const float2 *>(smem + stage * R::THETA_STAGE);
+    const uint8_t *sty = reinterpret_cast<const uint8_t *>(smem + stage * R::THETA_STAGE + R::T_TY);
     const int r0 = 2 * warp;
     const size_t cell0 = (size_t)(t.row + M + r0) * pitch + t.col + M + lane;
     const double mi0 = g.m[cell0], mi1 = g.m[cell0 + pitch];
     if (!mbar_wait_bounded(&bar[stage], (it >> 1) & 1, err)) return;
     float th[2];
     if (t.flags & kTileFull)
-      theta_tile32<M, true>(su, sl, sty, r0, lane, th);
+      theta_tile32<M, true>(su, sty, r0, lane, th);
     else
-      theta_tile32<M, false>(su, sl, sty, r0, lane, th);
+      theta_tile32<M, false>(su, sty, r0, lane, th);
     const double scale = 2.0 * P.dx * P.dy * P.dx;
 #pragma unroll
     for (int k = 0; k < 2; k++) {
@@ -337,7 +313,7 @@ __global__ void __launch_bounds__(kTileThreads, 3)
       p.v_np1[cell] = v;
       p.vh[cell] = vh2;
       p.u_np2[cell] = un;
-      split_store(p.u32_np2, p.l32_np2, cell, un);
+      p.u32_np2[cell] = make_float2((float)un.x, (float)un.y);
     }
     fence_proxy_async_smem();
     __syncthreads();
@@ -352,7 +328,7 @@ static void prepare32_m(DenseGroup &gr, int n_sm, cudaError_t *out) {
   using R = Region32<M>;
   cudaError_t e;
   *out = cudaSuccess;
-  if ((e = cudaFuncSetAttribute(k_theta32<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, Theta32<M>::SMEM)) ||
+  if ((e = cudaFuncSetAttribute(k_theta32<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, R::THETA_SMEM)) ||
       (e = cudaFuncSetAttribute(k_force32<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, R::FORCE_SMEM)) ||
       (e = cudaFuncSetAttribute(k_theta32<M>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                 cudaSharedmemCarveoutMaxShared)) ||
@@ -362,7 +338,7 @@ static void prepare32_m(DenseGroup &gr, int n_sm, cudaError_t *out) {
     return;
   }
   int bt = 0, bf = 0;
-  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, k_theta32<M>, kTileThreads, Theta32<M>::SMEM)) ||
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, k_theta32<M>, kTileThreads, R::THETA_SMEM)) ||
       (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf, k_force32<M>, kTileThreads, R::FORCE_SMEM))) {
     *out = e;
     return;
@@ -385,15 +361,15 @@ static void theta32_m(const DenseGroup &gr, const LaunchGeo &lg, const DenseGeo 
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(gr.grid_theta);
   cfg.blockDim = dim3(kTileThreads);
-  cfg.dynamicSmemBytes = Theta32<M>::SMEM;
+  cfg.dynamicSmemBytes = Region32<M>::THETA_SMEM;
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributePriority;
   attr[0].val.priority = dg.tile_priority;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  cudaLaunchKernelEx(&cfg, k_theta32<M>, gr.maps.u32[ring_u & 1], gr.maps.l32[ring_u & 1], gr.maps.type, lg.geo,
-                     dg.tiles, gr.tile_begin, gr.n_tiles, p, dg.pitch, skip_abc ? 1 : 0, gr.sched, dg.d_err);
+  cudaLaunchKernelEx(&cfg, k_theta32<M>, gr.maps.u32[ring_u & 1], gr.maps.type, lg.geo, dg.tiles, gr.tile_begin,
+                     gr.n_tiles, p, dg.pitch, skip_abc ? 1 : 0, gr.sched, dg.d_err);
 }
 
 template <int M>
