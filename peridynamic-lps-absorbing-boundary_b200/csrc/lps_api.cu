@@ -235,6 +235,8 @@ void fill_params(InstParams &P, const lps_problem &p, const lps_options &o, cons
   P.beta_lo = p.delta - p.dx / 2.0;
   P.beta_hi = p.delta + p.dx / 2.0;
   P.out_r = s.out_r;
+  P.f32_b0 = s.alpha;
+  P.f32_ab = (s.lam - s.mu) / (4.0 * s.mu);
   P.kinematic = o.kinematic_v;
   P.theta_method = o.theta_method;
   P.abcs_step = o.abcs_step;
@@ -479,6 +481,7 @@ int build_dense(lps_handle *h, const lps_problem *probs, const std::vector<Latti
   h->n_total = n;
   h->n_abc_total = total_abc;
   std::vector<double2> xy(n, make_double2(0, 0)), coef(n, make_double2(0, -1));
+  std::vector<float2> coef32(n, make_float2(0.f, -1.f));
   std::vector<uint8_t> type(n, 0);
   std::vector<int> abc_of(n, -1), blk_inst(n / kNodeBlock, 0);
   std::vector<double> m(n, 0.0);
@@ -503,7 +506,14 @@ int build_dense(lps_handle *h, const lps_problem *probs, const std::vector<Latti
       xy[c] = make_double2(p.nodes[2 * i], p.nodes[2 * i + 1]);
       type[c] = kExists | (p.bctypes[2 * i] == 1 ? kBcAbc : 0);
       m[c] = s.m[i];
-      if (s.m[i] > 0.0) coef[c] = make_double2(2.0 * (s.lam - s.mu) / s.m[i], 8.0 * s.mu / s.m[i]);
+      if (s.m[i] > 0.0) {
+        coef[c] = make_double2(2.0 * (s.lam - s.mu) / s.m[i], 8.0 * s.mu / s.m[i]);
+        // FP32-mixed form: both coefficients relative to their full-horizon
+        // values, m_ref / m_i -- exactly 1 wherever m_i = m_ref, so the
+        // material constants never round to FP32
+        const float q = (float)(s.m_ref / s.m[i]);
+        coef32[c] = make_float2(q, q);
+      }
     }
     for (int a = h->abc_begin[k]; a < h->abc_begin[k] + round_up(h->abc_count[k], kNodeBlock); a++) {
       H.inst[a] = k;
@@ -583,11 +593,7 @@ int build_dense(lps_handle *h, const lps_problem *probs, const std::vector<Latti
   G.len = nullptr; G.nbr = nullptr;
   D.tiles = d_tiles;
   D.fp32 = h->opt.precision == LPS_FP32_MIXED;
-  if (D.fp32) {
-    std::vector<float2> c32(n);
-    for (int c = 0; c < n; c++) c32[c] = make_float2((float)coef[c].x, (float)coef[c].y);
-    if ((st = dev_upload(h, &h->coef32, c32))) return st;
-  }
+  if (D.fp32 && (st = dev_upload(h, &h->coef32, coef32))) return st;
   if ((st = upload_abc(h, H, total_abc, abc_of))) return st;
   std::map<int, int> done;
   for (int k = 0; k < K; k++) {

@@ -22,7 +22,7 @@
 
 namespace lps {
 
-constexpr int kMaxInstances = 128;   // entries of the __constant__ table (176 B each)
+constexpr int kMaxInstances = 128;   // entries of the __constant__ table (192 B each)
 constexpr int kNodeBlock = 256;      // threads per node-kernel block
 constexpr int kAbcWarpsPerBlock = 8; // warps per ABC block (one ABC node each)
 
@@ -42,6 +42,8 @@ struct InstParams {
   double beta_lo;   // delta - dx/2         (:101)
   double beta_hi;   // delta + dx/2         (:103)
   double out_r;     // energy exclusion radius, <= 0: none (:528-530)
+  double f32_b0;    // FP32-mixed form: force scale alpha = 8 mu / m_ref (:485)
+  double f32_ab;    // FP32-mixed form: lambda_PD / alpha = (lambda - mu) / (4 mu)
   int node_begin, node_count;   // global node (or cell) range
   int abc_begin, abc_count;     // packed ABC list range
   int n_active_abc;             // entries with BCTypes == 1 (uB/vB denominators)

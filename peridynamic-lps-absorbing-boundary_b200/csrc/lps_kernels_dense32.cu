@@ -15,9 +15,11 @@
 // path dx = dy and delta = m dx, so with xi = dx (a, b), r = |(a, b)|,
 //   beta = 1 (r <= m - 1/2), m + 1/2 - r (r <= m + 1/2), 0    (:98-105)
 //   theta_i = (2 dx^3 / m_i) sum beta (a, b) . eta
-//   F_i     = dx^2 sum beta xi_hat [ (A'+ - A'-) r + (B_i + B+) e+ - (B_i + B-) e- ]
-// with A' = dx (2(l-m)/m) theta.  Each stencil column's partial sum is added
-// to the cell's total with Kahan compensation.
+//   F_i     = alpha dx^2 sum beta xi_hat [ (A'+ - A'-) r + (B'_i + B'+) e+ - (B'_i + B'-) e- ]
+// with B' = B / alpha = m_ref / m and A' = dx B' (lambda_PD / alpha) theta,
+// alpha = 8 mu / m_ref: material constants stay out of the FP32 arithmetic.
+// Each stencil column's partial sum is added to the cell's total with Kahan
+// compensation.
 #include <cmath>
 
 #include "lps_common.cuh"
@@ -223,8 +225,12 @@ __global__ void __launch_bounds__(kTileThreads, 2)
 
 // ---------------------------------------------------------------------------
 // Force (FP32) + corrector + next predictor (FP64), persistent over tiles.
-// After the copy lands, (theta, coef) become (A', B) = (dx 2(l-m)/m theta,
-// 8 mu/m) in the coef slot; absent neighbours and m <= 0 get A' = B = 0.
+// The FP32 sum is F / alpha with alpha = 8 mu / m_ref: coef32 holds
+// q = m_ref / m_i for both coefficients, so after the copy lands (theta, coef)
+// become (A', B') = (q (lambda_PD / alpha) theta dx, q) in the coef slot --
+// B' = 1 exactly at full-horizon nodes -- and the per-instance constants are
+// applied once, in FP64, to the finished sum.  Absent neighbours and m <= 0
+// get A' = B' = 0.
 template <int M>
 __global__ void __launch_bounds__(kTileThreads, 3)
     k_force32(const __grid_constant__ CUtensorMap map_u, const __grid_constant__ CUtensorMap map_th,
@@ -281,7 +287,7 @@ __global__ void __launch_bounds__(kTileThreads, 3)
       const int rr = q / R::RC, cc = q - rr * R::RC;
       const float2 co = sab[q];
       const bool valid = (sty[rr * R::RT + cc] & kExists) && co.y >= 0.f;
-      sab[q] = valid ? make_float2(co.x * (float)sth[q] * dxf, co.y) : make_float2(0.f, 0.f);
+      sab[q] = valid ? make_float2(co.x * (float)(sth[q] * P.f32_ab) * dxf, co.y) : make_float2(0.f, 0.f);
     }
     __syncthreads();
     float F[2][2];
@@ -289,7 +295,7 @@ __global__ void __launch_bounds__(kTileThreads, 3)
       force_tile32<M, true>(su, sab, r0, lane, F);
     else
       force_tile32<M, false>(su, sab, r0, lane, F);
-    const double scale = P.dx * P.dy / P.rho;
+    const double scale = P.f32_b0 * P.dx * P.dy / P.rho;
 #pragma unroll
     for (int k = 0; k < 2; k++) {
       const uint8_t ty = sty[(r0 + k + M) * R::RT + lane + M];
