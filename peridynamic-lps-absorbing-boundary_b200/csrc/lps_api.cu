@@ -810,6 +810,9 @@ int do_reset(lps_handle *h) {
     else
       launch_theta_csr(h->lg, h->U[0], h->TH[0], nullptr, nullptr, false, st);
   }
+  // dense path: G_theta runs a step ahead, so the first one runs here
+  if (h->path == LPS_PATH_DENSE && h->opt.theta_method == 1 && h->opt.abcs_step != -1)
+    launch_abc_theta_dense(h->lg, h->TH[0], h->TH[2], h->TH[1], st);
   // dense path: the force pass predicts the next level, so level 1 is
   // predicted here (src/main.cpp:727 with a^0 = 0)
   if (h->path == LPS_PATH_DENSE) launch_dense_reset_predict(h->lg, h->U0, h->V0, h->U[1], h->U32[1], h->VH, st);

@@ -105,14 +105,18 @@ void launch_theta32_group(const DenseGroup &gr, const LaunchGeo &lg, const Dense
                           int ring_u, bool skip_abc, cudaStream_t st);
 void launch_force32_group(const DenseGroup &gr, const LaunchGeo &lg, const DenseGeo &dg, const StepPtrs &p,
                           int ring_u, int ring_th, bool abc_on, bool first, int *d_step, cudaStream_t st);
-// One time step: theta tiles || G_theta, [IDW], force tiles; G_u/G_v runs
-// beside both tile passes.
+// One time step: theta tiles, [IDW], force tiles, ABC prediction; G_u/G_v
+// runs beside both tile passes, the next step's G_theta beside the force tiles.
 int enqueue_dense_step(const DenseGeo &dg, const LaunchGeo &lg, const StepPtrs &p, int *d_step,
                        cudaStream_t st, const Mark *mark, int ring_u);
 // Reset helpers: predicted u^1 (and its FP32 copy u32_1 when not null) and
 // vh for every cell from u^0, v^0.
 void launch_dense_reset_predict(const LaunchGeo &lg, const double2 *u0, const double2 *v0, double2 *u1,
                                 float2 *u32_1, double2 *vh, cudaStream_t st);
+// G_theta of the first step (theta^1 at ABC nodes from theta^0, theta^-1); the
+// dense step computes each later one a step ahead.
+void launch_abc_theta_dense(const LaunchGeo &lg, const double *th_n, const double *th_nm1, double *th_np1,
+                            cudaStream_t st);
 void launch_theta_dense_init(const DenseGeo &dg, const LaunchGeo &lg, const double2 *u, double *theta,
                              cudaStream_t st);
 void launch_diag_dense(const DenseGeo &dg, const LaunchGeo &lg, const double2 *u, const double2 *v,

@@ -698,26 +698,22 @@ int enqueue_dense_step(const DenseGeo &dg, const LaunchGeo &lg, const StepPtrs &
   // (serialised), so each kernel's device time can be read between events.
   const bool fork = mark == nullptr;
   cudaStream_t side = fork ? dg.side : st;
-  // pass 1: G_theta || predicted u -> theta tiles.  G_u/G_v follows G_theta
-  // on the side stream and runs on beside the force tiles: its results (the
-  // G_u buffer, v at ABC nodes) are read only by the next step's dilatation
-  // tiles and by the diagnostics, so the step joins it at its end.
+  // G_u/G_v of this step reads only the previous levels: it starts with the
+  // step on the side stream and runs beside both tile passes.  G_theta is one
+  // step ahead: theta^{n+2} at ABC nodes needs theta^{n+1} and theta^n only,
+  // so it follows the dilatation tiles on the side stream, beside the force
+  // tiles, into the ring slot that theta^{n-1} frees (the reset computes the
+  // first one).  The step joins the side stream at its end, before the ABC
+  // prediction that the next step's tiles read.
   const int n_blk = (lg.abc.n_abc + kAbcWarpsPerBlock - 1) / kAbcWarpsPerBlock;
   if (abc) {
     if (fork) {
       cudaEventRecord(dg.ev_fork[0], st);
       cudaStreamWaitEvent(side, dg.ev_fork[0], 0);
     }
-    if (gth) {
-      k_abc_theta<<<n_blk, 256, 0, side>>>(lg.abc, p.th_n, p.th_nm1, p.th_np1);
-      if (mark) (*mark)("abc_theta");
-      k++;
-    }
-    if (fork) cudaEventRecord(dg.ev_join[0], side);
     k_abc_uv_dense<<<n_blk, 256, 0, side>>>(lg.abc, p);
     if (mark) (*mark)("abc_uv");
     k++;
-    if (fork) cudaEventRecord(dg.ev_join[1], side);
   }
   for (const auto &gr : dg.groups) {
     if (dg.fp32)
@@ -726,13 +722,22 @@ int enqueue_dense_step(const DenseGeo &dg, const LaunchGeo &lg, const StepPtrs &
       LPS_DISPATCH_M(gr.m, launch_theta_group, gr, lg, dg, p, ring_u, gth, st);
     k++;
   }
-  if (abc && fork) cudaStreamWaitEvent(st, dg.ev_join[0], 0);
   if (mark) (*mark)("theta_tiles");
   if (abc && lg.theta_method == 0) {
     launch_theta_idw(lg, p.th_np1, st);
     if (mark) (*mark)("theta_idw");
     k++;
   }
+  if (gth) {
+    if (fork) {
+      cudaEventRecord(dg.ev_fork[1], st);
+      cudaStreamWaitEvent(side, dg.ev_fork[1], 0);
+    }
+    k_abc_theta<<<n_blk, 256, 0, side>>>(lg.abc, p.th_np1, p.th_n, const_cast<double *>(p.th_nm1));
+    if (mark) (*mark)("abc_theta");
+    k++;
+  }
+  if (abc && fork) cudaEventRecord(dg.ev_join[1], side);
   // pass 2: force tiles
   bool first = true;
   for (const auto &gr : dg.groups) {
@@ -756,6 +761,13 @@ int enqueue_dense_step(const DenseGeo &dg, const LaunchGeo &lg, const StepPtrs &
 void launch_dense_reset_predict(const LaunchGeo &lg, const double2 *u0, const double2 *v0, double2 *u1,
                                 float2 *u32_1, double2 *vh, cudaStream_t st) {
   k_dense_reset_predict<<<lg.n_node_blocks, 256, 0, st>>>(lg.geo, u0, v0, u1, u32_1, vh);
+}
+
+void launch_abc_theta_dense(const LaunchGeo &lg, const double *th_n, const double *th_nm1, double *th_np1,
+                            cudaStream_t st) {
+  if (lg.abc.n_abc == 0) return;
+  k_abc_theta<<<(lg.abc.n_abc + kAbcWarpsPerBlock - 1) / kAbcWarpsPerBlock, 256, 0, st>>>(lg.abc, th_n, th_nm1,
+                                                                                        th_np1);
 }
 
 void launch_theta_dense_init(const DenseGeo &, const LaunchGeo &lg, const double2 *u, double *theta,
