@@ -71,7 +71,7 @@ struct DenseGeo {
   int total_rows = 0;
   int tile_priority = 0;                       // launch priority of the tile kernels
   bool fp32 = false;                           // FP32-mixed tile kernels
-  int stream_grid = 0, stream_slots = 0, stream_cons = 0, stream_smem = 0;  // streaming ABC kernel
+  int stream_grid = 0, stream_slots = 0, stream_smem = 0;  // streaming ABC kernel
   cudaStream_t side = nullptr;                 // forked stream for the ABC kernels
   cudaEvent_t ev_fork[2] = {nullptr, nullptr}, ev_join[2] = {nullptr, nullptr};
   int *d_err = nullptr;                        // device wait-timeout flag

@@ -386,17 +386,14 @@ __global__ void __launch_bounds__(256) k_abc_predict(Abc ab, StepPtrs p) {
 // pairs): G_u and G_v of this step (src/main.cpp:883-916, :933-974) from u^n,
 // u^{n-1}, v^n, v^{n-1}, and G_theta one step ahead (:792-812): theta^{n+2}
 // from theta^{n+1}, theta^n into the ring slot that theta^{n-1} frees.
-// Ring protocol: the CTA's k-th block goes to slot k mod n_slots and to
-// consumer warp k mod n_cons; full[s] completes when a block has landed in
-// slot s, empty[s] when its consumer is done with it.  n_slots is a multiple
-// of n_cons, so every slot has one consumer warp, which takes the slot's
-// blocks in order -- a wait on a parity therefore never runs two phases
-// ahead of the barrier.  Every wait is bounded and raises the device error
-// flag.  Block size: 32 (n_cons + 1) threads, the last warp the producer.
-constexpr int kStreamWarps = 8;   // most consumer warps
+// Ring protocol: full[s] completes when block k (k = s mod n_slots) has
+// landed, empty[s] when its consumer is done with it; every wait is bounded
+// and raises the device error flag.
+constexpr int kStreamWarps = 8;
+constexpr int kStreamThreads = 32 * (kStreamWarps + 1);
 
-__global__ void __maxnreg__(80) k_abc_stream(Abc ab, StepPtrs p, int do_uv, int do_theta, int n_slots,
-                                             int n_cons, int slot_bytes, int *err) {
+__global__ void __maxnreg__(80) k_abc_stream(Abc ab, StepPtrs p, int do_uv, int do_theta,
+                                                              int n_slots, int slot_bytes, int *err) {
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t *full = reinterpret_cast<uint64_t *>(smem + (size_t)n_slots * slot_bytes);
   uint64_t *empty = full + n_slots;
@@ -411,7 +408,7 @@ __global__ void __maxnreg__(80) k_abc_stream(Abc ab, StepPtrs p, int do_uv, int 
   }
   __syncthreads();
   const int G = gridDim.x;
-  if (warp == n_cons) {  // producer
+  if (warp == kStreamWarps) {  // producer
     if (lane == 0)
       for (int k = 0;; k++) {
         const int e = blockIdx.x + k * G;
@@ -425,7 +422,7 @@ __global__ void __maxnreg__(80) k_abc_stream(Abc ab, StepPtrs p, int do_uv, int 
     return;
   }
   double *th_out = const_cast<double *>(p.th_nm1);
-  for (int k = warp;; k += n_cons) {
+  for (int k = warp;; k += kStreamWarps) {
     const int e = blockIdx.x + k * G;
     if (e >= ab.n_stream) break;
     const int slot = k % n_slots, use = k / n_slots;
@@ -727,9 +724,7 @@ cudaError_t dense_prepare(DenseGeo &dg, const Abc &ab, bool abc_on) {
   int budget = dg.fp32 ? smem_sm - 2 * (force_smem + reserve) - reserve : 200 * 1024;
   budget = std::min(budget, 200 * 1024);
   const int per_slot = ab.stream_slot_bytes + 16;
-  const int slots = std::max(1, std::min(16, budget / per_slot));
-  dg.stream_cons = std::min(kStreamWarps, slots);
-  dg.stream_slots = slots / dg.stream_cons * dg.stream_cons;  // a multiple of the consumer warps
+  dg.stream_slots = std::max(2, std::min(16, budget / per_slot));
   dg.stream_smem = dg.stream_slots * per_slot;
   dg.stream_grid = std::min(n_sm, ab.n_stream);
   cudaError_t e = cudaFuncSetAttribute(k_abc_stream, cudaFuncAttributeMaxDynamicSharedMemorySize, dg.stream_smem);
@@ -859,8 +854,8 @@ int enqueue_dense_step(const DenseGeo &dg, const LaunchGeo &lg, const StepPtrs &
       cudaEventRecord(dg.ev_fork[0], st);
       cudaStreamWaitEvent(side, dg.ev_fork[0], 0);
     }
-    k_abc_stream<<<dg.stream_grid, 32 * (dg.stream_cons + 1), dg.stream_smem, side>>>(
-        lg.abc, p, 1, gth ? 1 : 0, dg.stream_slots, dg.stream_cons, lg.abc.stream_slot_bytes, dg.d_err);
+    k_abc_stream<<<dg.stream_grid, kStreamThreads, dg.stream_smem, side>>>(
+        lg.abc, p, 1, gth ? 1 : 0, dg.stream_slots, lg.abc.stream_slot_bytes, dg.d_err);
     if (mark) (*mark)("abc_stream");
     k++;
     if (fork) cudaEventRecord(dg.ev_join[1], side);
