@@ -266,52 +266,6 @@ int upload_abc(lps_handle *h, const HostAbc &H, int total_abc, const std::vector
   return LPS_OK;
 }
 
-// Dense path: the operator blocks of the streaming ABC kernel (see Abc::blob).
-int upload_abc_stream(lps_handle *h, const HostAbc &H) {
-  Abc &B = h->lg.abc;
-  std::vector<unsigned char> blob;
-  std::vector<int2> ent;
-  std::vector<long long> off;
-  int max_bytes = 16;
-  std::vector<double> rows;
-  std::vector<int> idx;
-  for (size_t a = 0; a < H.writes.size(); a++) {
-    const int len = H.cl_len[a];
-    if (!H.writes[a]) continue;
-    const int l4 = std::max(4, (len + 3) / 4 * 4);
-    const size_t o = H.cl_off[a];
-    rows.assign((size_t)18 * l4, 0.0);
-    for (int r = 0; r < 8; r++)
-      for (int j = 0; j < len; j++) {
-        rows[(size_t)r * l4 + j] = H.gu[8 * o + (size_t)r * len + j];
-        rows[(size_t)(8 + r) * l4 + j] = H.gv[8 * o + (size_t)r * len + j];
-      }
-    for (int r = 0; r < 2; r++)
-      for (int j = 0; j < len; j++) rows[(size_t)(16 + r) * l4 + j] = H.gth[2 * o + (size_t)r * len + j];
-    idx.assign(l4, H.node[a]);
-    for (int j = 0; j < len; j++) idx[j] = H.cl_idx[o + j];
-    off.push_back((long long)blob.size());
-    ent.push_back(make_int2((int)a, l4));
-    const unsigned char *pr = reinterpret_cast<const unsigned char *>(rows.data());
-    const unsigned char *pi = reinterpret_cast<const unsigned char *>(idx.data());
-    blob.insert(blob.end(), pr, pr + sizeof(double) * rows.size());
-    blob.insert(blob.end(), pi, pi + sizeof(int) * idx.size());
-    max_bytes = std::max(max_bytes, 148 * l4);
-  }
-  unsigned char *d_blob;
-  int2 *d_ent;
-  long long *d_off;
-  int s;
-  if ((s = dev_upload(h, &d_blob, blob)) || (s = dev_upload(h, &d_ent, ent)) || (s = dev_upload(h, &d_off, off)))
-    return s;
-  B.blob = d_blob;
-  B.s_ent = d_ent;
-  B.s_off = d_off;
-  B.n_stream = (int)ent.size();
-  B.stream_slot_bytes = max_bytes;
-  return LPS_OK;
-}
-
 // ---------------------------------------------------------------------------
 int build_csr(lps_handle *h, const lps_problem *probs) {
   const int K = h->n_inst;
@@ -641,14 +595,13 @@ int build_dense(lps_handle *h, const lps_problem *probs, const std::vector<Latti
   D.fp32 = h->opt.precision == LPS_FP32_MIXED;
   if (D.fp32 && (st = dev_upload(h, &h->coef32, coef32))) return st;
   if ((st = upload_abc(h, H, total_abc, abc_of))) return st;
-  if ((st = upload_abc_stream(h, H))) return st;
   std::map<int, int> done;
   for (int k = 0; k < K; k++) {
     if (done.count(lat[k].M)) continue;
     done[lat[k].M] = 1;
     LPS_CUDA_TRY(h, upload_dense_constants(lat[k].M, probs[k].dx, probs[k].dy, probs[k].delta, h->stream));
   }
-  LPS_CUDA_TRY(h, dense_prepare(D, h->lg.abc, h->opt.abcs_step != -1 && total_abc > 0));
+  LPS_CUDA_TRY(h, dense_prepare(D));
   h->lg.n_node_blocks = n / kNodeBlock;
   h->lg.n_abc_blocks = total_abc / kAbcWarpsPerBlock;
   h->lg.n_inst = K;

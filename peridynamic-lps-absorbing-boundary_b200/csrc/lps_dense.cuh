@@ -59,7 +59,6 @@ struct DenseGroup {
   int n_tiles;
   int grid_theta;   // persistent grid sizes
   int grid_force;
-  int force_smem;   // dynamic shared memory of one force CTA
   int *sched;       // device tile-scheduler counters (theta: [0..1], force: [2..3])
   DenseMaps maps;
 };
@@ -71,7 +70,6 @@ struct DenseGeo {
   int total_rows = 0;
   int tile_priority = 0;                       // launch priority of the tile kernels
   bool fp32 = false;                           // FP32-mixed tile kernels
-  int stream_grid = 0, stream_slots = 0, stream_smem = 0;  // streaming ABC kernel
   cudaStream_t side = nullptr;                 // forked stream for the ABC kernels
   cudaEvent_t ev_fork[2] = {nullptr, nullptr}, ev_join[2] = {nullptr, nullptr};
   int *d_err = nullptr;                        // device wait-timeout flag
@@ -97,14 +95,12 @@ cudaError_t upload_dense_constants(int m, double dx, double dy, double delta, cu
 int dense_encode_maps(DenseGroup &g, int pitch, int total_rows, double2 *const *U, double *const *TH,
                       const double2 *coef, const uint8_t *type, float2 *const *U32, const float2 *coef32,
                       std::string &err);
-// Sets shared-memory limits and the persistent grid sizes of each group and
-// of the streaming absorbing-boundary kernel (ab: its blocks; abc_on: ABCs
-// are applied, so the FP32 force tiles leave room for it on every SM).
-cudaError_t dense_prepare(DenseGeo &dg, const Abc &ab, bool abc_on);
+// Sets shared-memory limits and the persistent grid sizes of each group.
+cudaError_t dense_prepare(DenseGeo &dg);
 
 // FP32-mixed tile kernels (lps_kernels_dense32.cu): shared-memory limits,
 // persistent grids and launches of one group.
-cudaError_t dense32_prepare_group(DenseGroup &gr, int n_sm, int max_force_ctas);
+cudaError_t dense32_prepare_group(DenseGroup &gr, int n_sm);
 void launch_theta32_group(const DenseGroup &gr, const LaunchGeo &lg, const DenseGeo &dg, const StepPtrs &p,
                           int ring_u, bool skip_abc, cudaStream_t st);
 void launch_force32_group(const DenseGroup &gr, const LaunchGeo &lg, const DenseGeo &dg, const StepPtrs &p,

@@ -106,16 +106,6 @@ struct Abc {
   const int *idw_off, *idw_len;// IDW neighbour lists (THETA_ABC_METHOD 0)
   const int *idw_idx;
   const double *idw_w;
-  // Dense path: the operators of each writing entry once more as one
-  // contiguous block for the streaming kernel -- G_u rows 0..7, G_v rows 0..7,
-  // G_theta rows 0..1 (len doubles each) then the cloud indices (len ints),
-  // len padded to a multiple of 4 with zero-weight entries on the node itself,
-  // so a block is 148 len bytes, a multiple of 16.
-  const unsigned char *blob;
-  const int2 *s_ent;           // (ABC entry, len) per block, blob order
-  const long long *s_off;      // byte offset of each block in blob
-  int n_stream;                // blocks
-  int stream_slot_bytes;       // largest block
 };
 
 // Per-block partial sums of the diagnostics (src/main.cpp:986-1062).

@@ -379,119 +379,6 @@ __global__ void __launch_bounds__(256) k_abc_predict(Abc ab, StepPtrs p) {
   if (p.u32_np2) p.u32_np2[node] = make_float2((float)up.x, (float)up.y);
 }
 
-// The absorbing boundary as a stream of operator blocks (Abc::blob): one
-// CTA per SM, a producer warp that keeps up to n_slots blocks in flight with
-// bulk copies into a shared-memory ring, and kStreamWarps consumer warps, one
-// block each at a time.  Per block (one writing ABC entry, lanes on entry
-// pairs): G_u and G_v of this step (src/main.cpp:883-916, :933-974) from u^n,
-// u^{n-1}, v^n, v^{n-1}, and G_theta one step ahead (:792-812): theta^{n+2}
-// from theta^{n+1}, theta^n into the ring slot that theta^{n-1} frees.
-// Ring protocol: full[s] completes when block k (k = s mod n_slots) has
-// landed, empty[s] when its consumer is done with it; every wait is bounded
-// and raises the device error flag.
-constexpr int kStreamWarps = 8;
-constexpr int kStreamThreads = 32 * (kStreamWarps + 1);
-
-__global__ void __maxnreg__(80) k_abc_stream(Abc ab, StepPtrs p, int do_uv, int do_theta,
-                                                              int n_slots, int slot_bytes, int *err) {
-  extern __shared__ __align__(128) unsigned char smem[];
-  uint64_t *full = reinterpret_cast<uint64_t *>(smem + (size_t)n_slots * slot_bytes);
-  uint64_t *empty = full + n_slots;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  if (*(volatile int *)err) return;
-  if (tid == 0) {
-    for (int i = 0; i < n_slots; i++) {
-      mbar_init(&full[i], 1);
-      mbar_init(&empty[i], 1);
-    }
-    mbar_fence_init();
-  }
-  __syncthreads();
-  const int G = gridDim.x;
-  if (warp == kStreamWarps) {  // producer
-    if (lane == 0)
-      for (int k = 0;; k++) {
-        const int e = blockIdx.x + k * G;
-        if (e >= ab.n_stream) break;
-        const int slot = k % n_slots, use = k / n_slots;
-        if (use > 0 && !mbar_wait_bounded(&empty[slot], (use - 1) & 1, err)) break;
-        const uint32_t bytes = 148u * (uint32_t)ab.s_ent[e].y;
-        mbar_expect_tx(&full[slot], bytes);
-        bulk_load(smem + (size_t)slot * slot_bytes, ab.blob + ab.s_off[e], bytes, &full[slot]);
-      }
-    return;
-  }
-  double *th_out = const_cast<double *>(p.th_nm1);
-  for (int k = warp;; k += kStreamWarps) {
-    const int e = blockIdx.x + k * G;
-    if (e >= ab.n_stream) break;
-    const int slot = k % n_slots, use = k / n_slots;
-    if (!mbar_wait_bounded(&full[slot], use & 1, err)) return;
-    const int2 ent = ab.s_ent[e];
-    const int a = ent.x, len = ent.y, hp = len >> 1;
-    const unsigned char *blk = smem + (size_t)slot * slot_bytes;
-    const double2 *gu = reinterpret_cast<const double2 *>(blk);
-    const double2 *gv = gu + 4 * len;
-    const double2 *gt = gv + 4 * len;
-    const int2 *idx = reinterpret_cast<const int2 *>(blk + 144 * len);
-    const InstParams &P = c_inst[ab.inst[a]];
-    const bool kin = P.kinematic != 0;
-    double ux = 0.0, uy = 0.0, vx = 0.0, vy = 0.0, th = 0.0;
-    for (int q = lane; q < hp; q += 32) {
-      const int2 kk = idx[q];
-      if (do_uv) {
-        const double2 un0 = p.u_n[kk.x], um0 = p.u_nm1[kk.x], un1 = p.u_n[kk.y], um1 = p.u_nm1[kk.y];
-        const double xs[4][2] = {{un0.x, un1.x}, {un0.y, un1.y}, {um0.x, um1.x}, {um0.y, um1.y}};
-#pragma unroll
-        for (int r = 0; r < 4; r++) {
-          const double2 gx = gu[r * hp + q], gy = gu[(4 + r) * hp + q];
-          ux += gx.x * xs[r][0] + gx.y * xs[r][1];
-          uy += gy.x * xs[r][0] + gy.y * xs[r][1];
-        }
-        if (!kin) {
-          const double2 vn0 = p.v_n[kk.x], vm0 = p.v_nm1[kk.x], vn1 = p.v_n[kk.y], vm1 = p.v_nm1[kk.y];
-          const double ys[4][2] = {{vn0.x, vn1.x}, {vn0.y, vn1.y}, {vm0.x, vm1.x}, {vm0.y, vm1.y}};
-#pragma unroll
-          for (int r = 0; r < 4; r++) {
-            const double2 hx = gv[r * hp + q], hy = gv[(4 + r) * hp + q];
-            vx += hx.x * ys[r][0] + hx.y * ys[r][1];
-            vy += hy.x * ys[r][0] + hy.y * ys[r][1];
-          }
-        }
-      }
-      if (do_theta) {
-        const double2 w0 = gt[q], w1 = gt[hp + q];
-        th += w0.x * p.th_np1[kk.x] + w0.y * p.th_np1[kk.y] + w1.x * p.th_n[kk.x] + w1.y * p.th_n[kk.y];
-      }
-    }
-    __syncwarp();
-    if (lane == 0) mbar_arrive(&empty[slot]);  // the block has been read
-    if (do_uv) {
-      ux = warp_sum(ux);
-      uy = warp_sum(uy);
-      if (!kin) {
-        vx = warp_sum(vx);
-        vy = warp_sum(vy);
-      }
-    }
-    if (do_theta) th = warp_sum(th);
-    if (lane == 0) {
-      const int node = ab.node[a];
-      if (do_uv) {
-        p.s_abc[a] = make_double2(ux, uy);
-        if (kin) {
-          // v = (u^{n+1} - u^n) / dt with this node's u^n, src/main.cpp:940-943
-          const double2 un = p.u_n[node];
-          p.v_np1[node] = make_double2((ux - un.x) / P.dt, (uy - un.y) / P.dt);
-        } else {
-          p.v_np1[node] = make_double2(vx, vy);
-        }
-      }
-      if (do_theta) th_out[node] = th;
-    }
-  }
-}
-
 // G_u (src/main.cpp:883-916) and G_v (:933-974) of one step for one ABC node
 // per warp, for the dense path.  u^n at ABC nodes is already in the ring (the
 // previous step's k_abc_predict merged it); the result goes to p.s_abc.
@@ -689,7 +576,6 @@ static cudaError_t prepare_m(DenseGroup &gr, int n_sm) {
   // absorbing-boundary kernel of the same step
   gr.grid_theta = std::min(gr.n_tiles, std::min(bt, 2) * n_sm);
   gr.grid_force = std::min(gr.n_tiles, bf * n_sm);
-  gr.force_smem = Region<M>::FORCE_SMEM;
   return cudaSuccess;
 }
 
@@ -698,39 +584,21 @@ static void prepare_dispatch(DenseGroup &gr, int n_sm, cudaError_t *e) {
   *e = prepare_m<M>(gr, n_sm);
 }
 
-cudaError_t dense_prepare(DenseGeo &dg, const Abc &ab, bool abc_on) {
-  int dev = 0, n_sm = 0, least = 0, greatest = 0, smem_sm = 0;
+cudaError_t dense_prepare(DenseGeo &dg) {
+  int dev = 0, n_sm = 0, least = 0, greatest = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-  cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
   cudaDeviceGetStreamPriorityRange(&least, &greatest);
   dg.tile_priority = greatest;  // tile CTAs are dispatched ahead of the ABC kernel's blocks
-  // FP32 force tiles at two CTAs per SM leave registers and shared memory for
-  // one CTA of the streaming ABC kernel beside them
-  const int force_ctas = abc_on ? 2 : 8;
-  int force_smem = 0;
   for (auto &gr : dg.groups) {
     cudaError_t e = cudaErrorInvalidValue;
     if (dg.fp32)
-      e = dense32_prepare_group(gr, n_sm, force_ctas);
+      e = dense32_prepare_group(gr, n_sm);
     else
       LPS_DISPATCH_M(gr.m, prepare_dispatch, gr, n_sm, &e);
     if (e != cudaSuccess) return e;
-    force_smem = std::max(force_smem, gr.force_smem);
   }
-  dg.stream_grid = dg.stream_slots = dg.stream_smem = 0;
-  if (!abc_on || ab.n_stream == 0) return cudaSuccess;
-  const int reserve = 1024;  // per-CTA shared memory the system keeps
-  int budget = dg.fp32 ? smem_sm - 2 * (force_smem + reserve) - reserve : 200 * 1024;
-  budget = std::min(budget, 200 * 1024);
-  const int per_slot = ab.stream_slot_bytes + 16;
-  dg.stream_slots = std::max(2, std::min(16, budget / per_slot));
-  dg.stream_smem = dg.stream_slots * per_slot;
-  dg.stream_grid = std::min(n_sm, ab.n_stream);
-  cudaError_t e = cudaFuncSetAttribute(k_abc_stream, cudaFuncAttributeMaxDynamicSharedMemorySize, dg.stream_smem);
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_abc_stream, cudaFuncAttributePreferredSharedMemoryCarveout,
-                              cudaSharedmemCarveoutMaxShared);
+  return cudaSuccess;
 }
 
 namespace {
@@ -830,12 +698,23 @@ int enqueue_dense_step(const DenseGeo &dg, const LaunchGeo &lg, const StepPtrs &
   // (serialised), so each kernel's device time can be read between events.
   const bool fork = mark == nullptr;
   cudaStream_t side = fork ? dg.side : st;
-  // The absorbing boundary is one streaming kernel after the dilatation
-  // tiles: G_u/G_v of this step and G_theta of the next (theta^{n+2} at ABC
-  // nodes from theta^{n+1}, theta^n, into the ring slot theta^{n-1} frees;
-  // the reset computes the first one).  It runs on the side stream beside
-  // the force tiles; the step joins it at its end, before the ABC prediction
-  // that the next step's tiles read.
+  // G_u/G_v of this step reads only the previous levels: it starts with the
+  // step on the side stream and runs beside both tile passes.  G_theta is one
+  // step ahead: theta^{n+2} at ABC nodes needs theta^{n+1} and theta^n only,
+  // so it follows the dilatation tiles on the side stream, beside the force
+  // tiles, into the ring slot that theta^{n-1} frees (the reset computes the
+  // first one).  The step joins the side stream at its end, before the ABC
+  // prediction that the next step's tiles read.
+  const int n_blk = (lg.abc.n_abc + kAbcWarpsPerBlock - 1) / kAbcWarpsPerBlock;
+  if (abc) {
+    if (fork) {
+      cudaEventRecord(dg.ev_fork[0], st);
+      cudaStreamWaitEvent(side, dg.ev_fork[0], 0);
+    }
+    k_abc_uv_dense<<<n_blk, 256, 0, side>>>(lg.abc, p);
+    if (mark) (*mark)("abc_uv");
+    k++;
+  }
   for (const auto &gr : dg.groups) {
     if (dg.fp32)
       launch_theta32_group(gr, lg, dg, p, ring_u, gth, st);
@@ -849,17 +728,16 @@ int enqueue_dense_step(const DenseGeo &dg, const LaunchGeo &lg, const StepPtrs &
     if (mark) (*mark)("theta_idw");
     k++;
   }
-  if (abc && dg.stream_grid > 0) {
+  if (gth) {
     if (fork) {
-      cudaEventRecord(dg.ev_fork[0], st);
-      cudaStreamWaitEvent(side, dg.ev_fork[0], 0);
+      cudaEventRecord(dg.ev_fork[1], st);
+      cudaStreamWaitEvent(side, dg.ev_fork[1], 0);
     }
-    k_abc_stream<<<dg.stream_grid, kStreamThreads, dg.stream_smem, side>>>(
-        lg.abc, p, 1, gth ? 1 : 0, dg.stream_slots, lg.abc.stream_slot_bytes, dg.d_err);
-    if (mark) (*mark)("abc_stream");
+    k_abc_theta<<<n_blk, 256, 0, side>>>(lg.abc, p.th_np1, p.th_n, const_cast<double *>(p.th_nm1));
+    if (mark) (*mark)("abc_theta");
     k++;
-    if (fork) cudaEventRecord(dg.ev_join[1], side);
   }
+  if (abc && fork) cudaEventRecord(dg.ev_join[1], side);
   // pass 2: force tiles
   bool first = true;
   for (const auto &gr : dg.groups) {
@@ -872,7 +750,7 @@ int enqueue_dense_step(const DenseGeo &dg, const LaunchGeo &lg, const StepPtrs &
   }
   if (mark) (*mark)("force_tiles");
   if (abc) {
-    if (fork && dg.stream_grid > 0) cudaStreamWaitEvent(st, dg.ev_join[1], 0);
+    if (fork) cudaStreamWaitEvent(st, dg.ev_join[1], 0);
     k_abc_predict<<<(lg.abc.n_abc + 255) / 256, 256, 0, st>>>(lg.abc, p);
     if (mark) (*mark)("abc_predict");
     k++;

@@ -330,7 +330,7 @@ __global__ void __launch_bounds__(kTileThreads, 3)
 // ---------------------------------------------------------------------------
 // host side
 template <int M>
-static void prepare32_m(DenseGroup &gr, int n_sm, int max_force_ctas, cudaError_t *out) {
+static void prepare32_m(DenseGroup &gr, int n_sm, cudaError_t *out) {
   using R = Region32<M>;
   cudaError_t e;
   *out = cudaSuccess;
@@ -350,15 +350,14 @@ static void prepare32_m(DenseGroup &gr, int n_sm, int max_force_ctas, cudaError_
     return;
   }
   bt = std::max(bt, 1);
-  bf = std::max(1, std::min(bf, max_force_ctas));
-  gr.force_smem = R::FORCE_SMEM;
+  bf = std::max(bf, 1);
   gr.grid_theta = std::min(gr.n_tiles, bt * n_sm);
   gr.grid_force = std::min(gr.n_tiles, bf * n_sm);
 }
 
-cudaError_t dense32_prepare_group(DenseGroup &gr, int n_sm, int max_force_ctas) {
+cudaError_t dense32_prepare_group(DenseGroup &gr, int n_sm) {
   cudaError_t e = cudaErrorInvalidValue;
-  LPS_DISPATCH_M(gr.m, prepare32_m, gr, n_sm, max_force_ctas, &e);
+  LPS_DISPATCH_M(gr.m, prepare32_m, gr, n_sm, &e);
   return e;
 }
 
