@@ -106,6 +106,11 @@ struct Abc {
   const int *idw_off, *idw_len;// IDW neighbour lists (THETA_ABC_METHOD 0)
   const int *idw_idx;
   const double *idw_w;
+  // Dense path: one record per writing entry for the pipelined kernel --
+  // (cloud offset, cloud length, node, entry | instance << 24).
+  const int4 *recs;
+  int n_recs;
+  int pad_;
 };
 
 // Per-block partial sums of the diagnostics (src/main.cpp:986-1062).

@@ -1,12 +1,15 @@
 // lps_kernels_dense.cu -- masked dense-grid stencil kernels, FP64, sm_100a.
 //
 // One time step is two persistent tile kernels on the main stream and the
-// absorbing-boundary kernels on a forked stream:
+// absorbing-boundary kernels:
 //   k_theta_tma<M>   dilatation (src/main.cpp:736-761) of the predicted
-//                    displacements      || k_abc_theta: G_theta (:792-812)
+//                    displacements
 //   k_force_tma<M>   force (:821-874), corrector (:922-925) and the next
 //                    step's predictor (:725-728)
-//   k_abc_uv_dense   G_u, G_v (:883-916, :933-974), beside both tile passes
+//   k_abc_pipe       G_u, G_v (:883-916, :933-974) of the step and G_theta
+//                    (:792-812) of the next, on a side stream beside the force
+//                    tiles
+//   k_abc_predict    the ABC nodes' merge and prediction at the end of the step
 // Tile kernels stage a 16 x 32 tile plus its m-cell halo with TMA
 // (cp.async.bulk.tensor) into one of two shared-memory buffers while the
 // other buffer is being computed; every wait on the transaction barrier is
@@ -346,15 +349,97 @@ __global__ void __launch_bounds__(kTileThreads, 2)
 }
 
 // ---------------------------------------------------------------------------
-// Absorbing-boundary kernels (run concurrently with the tile kernels).
-__global__ void __launch_bounds__(256) k_abc_theta(Abc ab, const double *th_n, const double *th_nm1, double *theta) {
-  const int a = blockIdx.x * kAbcWarpsPerBlock + (threadIdx.x >> 5);
-  abc_theta_warp(ab, a, th_n, th_nm1, theta);
-}
-
-__global__ void __launch_bounds__(256) k_abc_uv(Abc ab, StepPtrs p) {
-  const int a = blockIdx.x * kAbcWarpsPerBlock + (threadIdx.x >> 5);
-  abc_uv_warp(ab, a, p);
+// Absorbing-boundary kernels of the dense path.
+// The absorbing boundary of a dense step, software-pipelined: a persistent
+// warp walks the writing entries i, i + W, ... (W warps in the grid) and
+// loads the record of entry i + 2W and the cloud indices of entry i + W while
+// it works on entry i, so the operator rows and the gathered state of an
+// entry are its only memory round trip.  Per entry (lanes on cloud entries):
+// G_u and G_v of this step (src/main.cpp:883-916, :933-974) from u^n,
+// u^{n-1}, v^n, v^{n-1}, and, one step ahead, G_theta (:792-812): theta^{n+2}
+// from theta^{n+1} (p.th_np1) and theta^n (p.th_n) into the ring slot that
+// theta^{n-1} (p.th_nm1) frees.  Clouds longer than 64 entries load their
+// further indices in the loop.
+__global__ void __launch_bounds__(256, 3) k_abc_pipe(Abc ab, StepPtrs p, int do_uv, int do_theta) {
+  const int lane = threadIdx.x & 31;
+  const int W = gridDim.x * kAbcWarpsPerBlock;
+  const int n = ab.n_recs;
+  int i = blockIdx.x * kAbcWarpsPerBlock + (threadIdx.x >> 5);
+  if (i >= n) return;
+  double *th_out = const_cast<double *>(p.th_nm1);
+  const int4 z4 = make_int4(0, 0, 0, 0);
+  int4 rec = ab.recs[i];
+  int4 rec_next = i + W < n ? ab.recs[i + W] : z4;
+  int ka = lane < rec.y ? __ldg(ab.cl_idx + rec.x + lane) : 0;
+  int kb = 32 + lane < rec.y ? __ldg(ab.cl_idx + rec.x + 32 + lane) : 0;
+  while (true) {
+    // prefetch: cloud indices of the next entry, record of the one after
+    const int ka_n = lane < rec_next.y ? __ldg(ab.cl_idx + rec_next.x + lane) : 0;
+    const int kb_n = 32 + lane < rec_next.y ? __ldg(ab.cl_idx + rec_next.x + 32 + lane) : 0;
+    const int4 rec_nn = i + 2 * W < n ? ab.recs[i + 2 * W] : z4;
+    const int off = rec.x, len = rec.y, node = rec.z, a = rec.w & 0xffffff;
+    const InstParams &P = c_inst[rec.w >> 24];
+    const bool kin = P.kinematic != 0;
+    const double *__restrict__ gu = ab.gu + 8 * (size_t)off;
+    const double *__restrict__ gv = ab.gv + 8 * (size_t)off;
+    const double *__restrict__ w0 = ab.gth + 2 * (size_t)off;
+    const double *__restrict__ w1 = w0 + len;
+    double ux = 0.0, uy = 0.0, vx = 0.0, vy = 0.0, th = 0.0;
+    const double2 z = make_double2(0.0, 0.0);
+    for (int e0 = 0; e0 < len; e0 += 64) {
+      const int ea = e0 + lane, eb = e0 + 32 + lane;
+      const bool va = ea < len, vb = eb < len;
+      int ia = ka, ib = kb;
+      if (e0 > 0) {
+        ia = va ? __ldg(ab.cl_idx + off + ea) : 0;
+        ib = vb ? __ldg(ab.cl_idx + off + eb) : 0;
+      }
+      if (do_uv) {
+        const double2 una = va ? p.u_n[ia] : z, uma = va ? p.u_nm1[ia] : z;
+        const double2 unb = vb ? p.u_n[ib] : z, umb = vb ? p.u_nm1[ib] : z;
+        if (va) g_entry(gu, len, ea, una, uma, ux, uy);
+        if (vb) g_entry(gu, len, eb, unb, umb, ux, uy);
+        if (!kin) {
+          const double2 vna = va ? p.v_n[ia] : z, vma = va ? p.v_nm1[ia] : z;
+          const double2 vnb = vb ? p.v_n[ib] : z, vmb = vb ? p.v_nm1[ib] : z;
+          if (va) g_entry(gv, len, ea, vna, vma, vx, vy);
+          if (vb) g_entry(gv, len, eb, vnb, vmb, vx, vy);
+        }
+      }
+      if (do_theta) {
+        if (va) th += __ldg(w0 + ea) * p.th_np1[ia] + __ldg(w1 + ea) * p.th_n[ia];
+        if (vb) th += __ldg(w0 + eb) * p.th_np1[ib] + __ldg(w1 + eb) * p.th_n[ib];
+      }
+    }
+    if (do_uv) {
+      ux = warp_sum(ux);
+      uy = warp_sum(uy);
+      if (!kin) {
+        vx = warp_sum(vx);
+        vy = warp_sum(vy);
+      }
+    }
+    if (do_theta) th = warp_sum(th);
+    if (lane == 0) {
+      if (do_uv) {
+        p.s_abc[a] = make_double2(ux, uy);
+        if (kin) {
+          // v = (u^{n+1} - u^n) / dt with this node's u^n, src/main.cpp:940-943
+          const double2 un = p.u_n[node];
+          p.v_np1[node] = make_double2((ux - un.x) / P.dt, (uy - un.y) / P.dt);
+        } else {
+          p.v_np1[node] = make_double2(vx, vy);
+        }
+      }
+      if (do_theta) th_out[node] = th;
+    }
+    i += W;
+    if (i >= n) break;
+    rec = rec_next;
+    rec_next = rec_nn;
+    ka = ka_n;
+    kb = kb_n;
+  }
 }
 
 // End of a dense step at the absorbing boundary, after the force tiles and
@@ -377,54 +462,6 @@ __global__ void __launch_bounds__(256) k_abc_predict(Abc ab, StepPtrs p) {
   p.u_np2[node] = up;
   p.vh[node] = vh;
   if (p.u32_np2) p.u32_np2[node] = make_float2((float)up.x, (float)up.y);
-}
-
-// G_u (src/main.cpp:883-916) and G_v (:933-974) of one step for one ABC node
-// per warp, for the dense path.  u^n at ABC nodes is already in the ring (the
-// previous step's k_abc_predict merged it); the result goes to p.s_abc.
-__global__ void __launch_bounds__(256) k_abc_uv_dense(Abc ab, StepPtrs p) {
-  const int lane = threadIdx.x & 31;
-  const int a = blockIdx.x * kAbcWarpsPerBlock + (threadIdx.x >> 5);
-  if (a >= ab.n_abc || !ab.writes[a]) return;
-  const InstParams &P = c_inst[ab.inst[a]];
-  const int off = ab.cl_off[a], len = ab.cl_len[a];
-  const double *__restrict__ gu = ab.gu + 8 * (size_t)off;
-  const double *__restrict__ gv = ab.gv + 8 * (size_t)off;
-  const bool kin = P.kinematic != 0;
-  double ux = 0.0, uy = 0.0, vx = 0.0, vy = 0.0;
-  const double2 z = make_double2(0.0, 0.0);
-  for (int e0 = 0; e0 < len; e0 += 64) {
-    const int ea = e0 + lane, eb = e0 + 32 + lane;
-    const bool va = ea < len, vb = eb < len;
-    const int ka = va ? __ldg(ab.cl_idx + off + ea) : 0, kb = vb ? __ldg(ab.cl_idx + off + eb) : 0;
-    const double2 una = va ? p.u_n[ka] : z, uma = va ? p.u_nm1[ka] : z;
-    const double2 unb = vb ? p.u_n[kb] : z, umb = vb ? p.u_nm1[kb] : z;
-    if (va) g_entry(gu, len, ea, una, uma, ux, uy);
-    if (vb) g_entry(gu, len, eb, unb, umb, ux, uy);
-    if (!kin) {
-      const double2 vna = va ? p.v_n[ka] : z, vma = va ? p.v_nm1[ka] : z;
-      const double2 vnb = vb ? p.v_n[kb] : z, vmb = vb ? p.v_nm1[kb] : z;
-      if (va) g_entry(gv, len, ea, vna, vma, vx, vy);
-      if (vb) g_entry(gv, len, eb, vnb, vmb, vx, vy);
-    }
-  }
-  ux = warp_sum(ux);
-  uy = warp_sum(uy);
-  if (!kin) {
-    vx = warp_sum(vx);
-    vy = warp_sum(vy);
-  }
-  if (lane == 0) {
-    const int node = ab.node[a];
-    p.s_abc[a] = make_double2(ux, uy);
-    if (kin) {
-      // v = (u^{n+1} - u^n) / dt with this node's u^n, src/main.cpp:940-943
-      const double2 un = p.u_n[node];
-      p.v_np1[node] = make_double2((ux - un.x) / P.dt, (uy - un.y) / P.dt);
-    } else {
-      p.v_np1[node] = make_double2(vx, vy);
-    }
-  }
 }
 
 // ---------------------------------------------------------------------------
@@ -584,7 +621,7 @@ static void prepare_dispatch(DenseGroup &gr, int n_sm, cudaError_t *e) {
   *e = prepare_m<M>(gr, n_sm);
 }
 
-cudaError_t dense_prepare(DenseGeo &dg) {
+cudaError_t dense_prepare(DenseGeo &dg, const Abc &ab) {
   int dev = 0, n_sm = 0, least = 0, greatest = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
@@ -598,6 +635,11 @@ cudaError_t dense_prepare(DenseGeo &dg) {
       LPS_DISPATCH_M(gr.m, prepare_dispatch, gr, n_sm, &e);
     if (e != cudaSuccess) return e;
   }
+  int per_sm = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_abc_pipe, 256, 0);
+  if (e != cudaSuccess) return e;
+  const int need = (ab.n_recs + kAbcWarpsPerBlock - 1) / kAbcWarpsPerBlock;
+  dg.abc_grid = std::max(1, std::min(need, std::max(per_sm, 1) * n_sm));
   return cudaSuccess;
 }
 
@@ -698,23 +740,12 @@ int enqueue_dense_step(const DenseGeo &dg, const LaunchGeo &lg, const StepPtrs &
   // (serialised), so each kernel's device time can be read between events.
   const bool fork = mark == nullptr;
   cudaStream_t side = fork ? dg.side : st;
-  // G_u/G_v of this step reads only the previous levels: it starts with the
-  // step on the side stream and runs beside both tile passes.  G_theta is one
-  // step ahead: theta^{n+2} at ABC nodes needs theta^{n+1} and theta^n only,
-  // so it follows the dilatation tiles on the side stream, beside the force
-  // tiles, into the ring slot that theta^{n-1} frees (the reset computes the
-  // first one).  The step joins the side stream at its end, before the ABC
-  // prediction that the next step's tiles read.
-  const int n_blk = (lg.abc.n_abc + kAbcWarpsPerBlock - 1) / kAbcWarpsPerBlock;
-  if (abc) {
-    if (fork) {
-      cudaEventRecord(dg.ev_fork[0], st);
-      cudaStreamWaitEvent(side, dg.ev_fork[0], 0);
-    }
-    k_abc_uv_dense<<<n_blk, 256, 0, side>>>(lg.abc, p);
-    if (mark) (*mark)("abc_uv");
-    k++;
-  }
+  // The absorbing boundary is one pipelined kernel after the dilatation
+  // tiles: G_u/G_v of this step and G_theta of the next (theta^{n+2} at ABC
+  // nodes from theta^{n+1}, theta^n, into the ring slot theta^{n-1} frees;
+  // the reset computes the first one).  It runs on the side stream beside the
+  // force tiles; the step joins it at its end, before the ABC prediction that
+  // the next step's tiles read.
   for (const auto &gr : dg.groups) {
     if (dg.fp32)
       launch_theta32_group(gr, lg, dg, p, ring_u, gth, st);
@@ -728,16 +759,17 @@ int enqueue_dense_step(const DenseGeo &dg, const LaunchGeo &lg, const StepPtrs &
     if (mark) (*mark)("theta_idw");
     k++;
   }
-  if (gth) {
+  const bool pipe = abc && lg.abc.n_recs > 0;
+  if (pipe) {
     if (fork) {
-      cudaEventRecord(dg.ev_fork[1], st);
-      cudaStreamWaitEvent(side, dg.ev_fork[1], 0);
+      cudaEventRecord(dg.ev_fork[0], st);
+      cudaStreamWaitEvent(side, dg.ev_fork[0], 0);
     }
-    k_abc_theta<<<n_blk, 256, 0, side>>>(lg.abc, p.th_np1, p.th_n, const_cast<double *>(p.th_nm1));
-    if (mark) (*mark)("abc_theta");
+    k_abc_pipe<<<dg.abc_grid, 256, 0, side>>>(lg.abc, p, 1, gth ? 1 : 0);
+    if (mark) (*mark)("abc_pipe");
     k++;
+    if (fork) cudaEventRecord(dg.ev_join[1], side);
   }
-  if (abc && fork) cudaEventRecord(dg.ev_join[1], side);
   // pass 2: force tiles
   bool first = true;
   for (const auto &gr : dg.groups) {
@@ -750,7 +782,7 @@ int enqueue_dense_step(const DenseGeo &dg, const LaunchGeo &lg, const StepPtrs &
   }
   if (mark) (*mark)("force_tiles");
   if (abc) {
-    if (fork) cudaStreamWaitEvent(st, dg.ev_join[1], 0);
+    if (fork && pipe) cudaStreamWaitEvent(st, dg.ev_join[1], 0);
     k_abc_predict<<<(lg.abc.n_abc + 255) / 256, 256, 0, st>>>(lg.abc, p);
     if (mark) (*mark)("abc_predict");
     k++;
@@ -763,11 +795,14 @@ void launch_dense_reset_predict(const LaunchGeo &lg, const double2 *u0, const do
   k_dense_reset_predict<<<lg.n_node_blocks, 256, 0, st>>>(lg.geo, u0, v0, u1, u32_1, vh);
 }
 
-void launch_abc_theta_dense(const LaunchGeo &lg, const double *th_n, const double *th_nm1, double *th_np1,
-                            cudaStream_t st) {
-  if (lg.abc.n_abc == 0) return;
-  k_abc_theta<<<(lg.abc.n_abc + kAbcWarpsPerBlock - 1) / kAbcWarpsPerBlock, 256, 0, st>>>(lg.abc, th_n, th_nm1,
-                                                                                        th_np1);
+void launch_abc_theta_dense(const DenseGeo &dg, const LaunchGeo &lg, const double *th_n, const double *th_nm1,
+                            double *th_np1, cudaStream_t st) {
+  if (lg.abc.n_recs == 0) return;
+  StepPtrs p = {};
+  p.th_np1 = const_cast<double *>(th_n);  // the kernel's "newer" level
+  p.th_n = th_nm1;
+  p.th_nm1 = th_np1;                       // output slot
+  k_abc_pipe<<<dg.abc_grid, 256, 0, st>>>(lg.abc, p, 0, 1);
 }
 
 void launch_theta_dense_init(const DenseGeo &, const LaunchGeo &lg, const double2 *u, double *theta,
