@@ -350,95 +350,90 @@ __global__ void __launch_bounds__(kTileThreads, 2)
 
 // ---------------------------------------------------------------------------
 // Absorbing-boundary kernels of the dense path.
-// The absorbing boundary of a dense step, software-pipelined: a persistent
-// warp walks the writing entries i, i + W, ... (W warps in the grid) and
-// loads the record of entry i + 2W and the cloud indices of entry i + W while
-// it works on entry i, so the operator rows and the gathered state of an
-// entry are its only memory round trip.  Per entry (lanes on cloud entries):
-// G_u and G_v of this step (src/main.cpp:883-916, :933-974) from u^n,
-// u^{n-1}, v^n, v^{n-1}, and, one step ahead, G_theta (:792-812): theta^{n+2}
-// from theta^{n+1} (p.th_np1) and theta^n (p.th_n) into the ring slot that
-// theta^{n-1} (p.th_nm1) frees.  Clouds longer than 64 entries load their
-// further indices in the loop.
+// One cloud entry's contribution to the x and y outputs of a 2-level operator
+// (rows component-major, len doubles each), with streaming loads: the
+// operators are read once per step, so they should not push the gathered
+// state out of L2.
+__device__ __forceinline__ void g_entry_stream(const double *__restrict__ g, int len, int e, double2 xn, double2 xm,
+                                               double &ox, double &oy) {
+  ox += __ldcs(g + 0 * len + e) * xn.x + __ldcs(g + 1 * len + e) * xn.y + __ldcs(g + 2 * len + e) * xm.x +
+        __ldcs(g + 3 * len + e) * xm.y;
+  oy += __ldcs(g + 4 * len + e) * xn.x + __ldcs(g + 5 * len + e) * xn.y + __ldcs(g + 6 * len + e) * xm.x +
+        __ldcs(g + 7 * len + e) * xm.y;
+}
+
+// The absorbing boundary of a dense step, software-pipelined over a warp
+// pair per entry: a persistent pair of warps walks the writing entries
+// i, i + P, ... (P pairs in the grid); each warp takes every other 32 cloud
+// entries of an entry, one per lane, so a lane keeps the operator rows and the
+// gathered state of a single cloud entry in flight at once, and it loads the
+// record of entry i + 2P and its cloud indices of entry i + P while it works
+// on entry i.  The odd warp hands its partial sums to the even one through
+// shared memory (a 64-thread named barrier per pair).  Per entry: G_u and G_v
+// of this step (src/main.cpp:883-916, :933-974) from u^n, u^{n-1}, v^n,
+// v^{n-1}, and, one step ahead, G_theta (:792-812): theta^{n+2} from
+// theta^{n+1} (p.th_np1) and theta^n (p.th_n) into the ring slot that
+// theta^{n-1} (p.th_nm1) frees.
 __global__ void __launch_bounds__(256, 3) k_abc_pipe(Abc ab, StepPtrs p, int do_uv, int do_theta) {
-  const int lane = threadIdx.x & 31;
-  const int W = gridDim.x * kAbcWarpsPerBlock;
+  __shared__ double part[2][kAbcWarpsPerBlock / 2][5];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, half = wib & 1, pib = wib >> 1;
+  const int P = gridDim.x * (kAbcWarpsPerBlock / 2);
   const int n = ab.n_recs;
-  int i = blockIdx.x * kAbcWarpsPerBlock + (threadIdx.x >> 5);
-  if (i >= n) return;
+  int i = blockIdx.x * (kAbcWarpsPerBlock / 2) + pib;
+  if (i >= n) return;  // both warps of the pair leave together
   double *th_out = const_cast<double *>(p.th_nm1);
   const int4 z4 = make_int4(0, 0, 0, 0);
+  const int e_first = 32 * half + lane;  // this lane's first cloud entry; then every 64
   int4 rec = ab.recs[i];
-  int4 rec_next = i + W < n ? ab.recs[i + W] : z4;
-  int ka = lane < rec.y ? __ldg(ab.cl_idx + rec.x + lane) : 0;
-  int kb = 32 + lane < rec.y ? __ldg(ab.cl_idx + rec.x + 32 + lane) : 0;
-  while (true) {
-    // prefetch: cloud indices of the next entry, record of the one after
-    const int ka_n = lane < rec_next.y ? __ldg(ab.cl_idx + rec_next.x + lane) : 0;
-    const int kb_n = 32 + lane < rec_next.y ? __ldg(ab.cl_idx + rec_next.x + 32 + lane) : 0;
-    const int4 rec_nn = i + 2 * W < n ? ab.recs[i + 2 * W] : z4;
+  int4 rec_next = i + P < n ? ab.recs[i + P] : z4;
+  int k_cur = e_first < rec.y ? __ldg(ab.cl_idx + rec.x + e_first) : 0;
+  for (int it = 0;; it++) {
+    // prefetch: this lane's first cloud index of the next entry, record of the one after
+    const int k_next = e_first < rec_next.y ? __ldg(ab.cl_idx + rec_next.x + e_first) : 0;
+    const int4 rec_nn = i + 2 * P < n ? ab.recs[i + 2 * P] : z4;
     const int off = rec.x, len = rec.y, node = rec.z, a = rec.w & 0xffffff;
-    const InstParams &P = c_inst[rec.w >> 24];
-    const bool kin = P.kinematic != 0;
+    const InstParams &Pi = c_inst[rec.w >> 24];
+    const bool kin = Pi.kinematic != 0;
     const double *__restrict__ gu = ab.gu + 8 * (size_t)off;
     const double *__restrict__ gv = ab.gv + 8 * (size_t)off;
     const double *__restrict__ w0 = ab.gth + 2 * (size_t)off;
     const double *__restrict__ w1 = w0 + len;
-    double ux = 0.0, uy = 0.0, vx = 0.0, vy = 0.0, th = 0.0;
-    const double2 z = make_double2(0.0, 0.0);
-    for (int e0 = 0; e0 < len; e0 += 64) {
-      const int ea = e0 + lane, eb = e0 + 32 + lane;
-      const bool va = ea < len, vb = eb < len;
-      int ia = ka, ib = kb;
-      if (e0 > 0) {
-        ia = va ? __ldg(ab.cl_idx + off + ea) : 0;
-        ib = vb ? __ldg(ab.cl_idx + off + eb) : 0;
-      }
+    double s[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // ux, uy, vx, vy, theta
+    for (int e = e_first; e < len; e += 64) {
+      const int k = e == e_first ? k_cur : __ldg(ab.cl_idx + off + e);
       if (do_uv) {
-        const double2 una = va ? p.u_n[ia] : z, uma = va ? p.u_nm1[ia] : z;
-        const double2 unb = vb ? p.u_n[ib] : z, umb = vb ? p.u_nm1[ib] : z;
-        if (va) g_entry(gu, len, ea, una, uma, ux, uy);
-        if (vb) g_entry(gu, len, eb, unb, umb, ux, uy);
-        if (!kin) {
-          const double2 vna = va ? p.v_n[ia] : z, vma = va ? p.v_nm1[ia] : z;
-          const double2 vnb = vb ? p.v_n[ib] : z, vmb = vb ? p.v_nm1[ib] : z;
-          if (va) g_entry(gv, len, ea, vna, vma, vx, vy);
-          if (vb) g_entry(gv, len, eb, vnb, vmb, vx, vy);
-        }
+        g_entry_stream(gu, len, e, p.u_n[k], p.u_nm1[k], s[0], s[1]);
+        if (!kin) g_entry_stream(gv, len, e, p.v_n[k], p.v_nm1[k], s[2], s[3]);
       }
-      if (do_theta) {
-        if (va) th += __ldg(w0 + ea) * p.th_np1[ia] + __ldg(w1 + ea) * p.th_n[ia];
-        if (vb) th += __ldg(w0 + eb) * p.th_np1[ib] + __ldg(w1 + eb) * p.th_n[ib];
-      }
+      if (do_theta) s[4] += __ldcs(w0 + e) * p.th_np1[k] + __ldcs(w1 + e) * p.th_n[k];
     }
-    if (do_uv) {
-      ux = warp_sum(ux);
-      uy = warp_sum(uy);
-      if (!kin) {
-        vx = warp_sum(vx);
-        vy = warp_sum(vy);
-      }
-    }
-    if (do_theta) th = warp_sum(th);
-    if (lane == 0) {
+#pragma unroll
+    for (int j = 0; j < 5; j++) s[j] = warp_sum(s[j]);
+    double(*buf)[5] = part[it & 1];
+    if (half == 1 && lane == 0)
+#pragma unroll
+      for (int j = 0; j < 5; j++) buf[pib][j] = s[j];
+    asm volatile("bar.sync %0, 64;" ::"r"(1 + pib) : "memory");
+    if (half == 0 && lane == 0) {
+#pragma unroll
+      for (int j = 0; j < 5; j++) s[j] += buf[pib][j];
       if (do_uv) {
-        p.s_abc[a] = make_double2(ux, uy);
+        p.s_abc[a] = make_double2(s[0], s[1]);
         if (kin) {
           // v = (u^{n+1} - u^n) / dt with this node's u^n, src/main.cpp:940-943
           const double2 un = p.u_n[node];
-          p.v_np1[node] = make_double2((ux - un.x) / P.dt, (uy - un.y) / P.dt);
+          p.v_np1[node] = make_double2((s[0] - un.x) / Pi.dt, (s[1] - un.y) / Pi.dt);
         } else {
-          p.v_np1[node] = make_double2(vx, vy);
+          p.v_np1[node] = make_double2(s[2], s[3]);
         }
       }
-      if (do_theta) th_out[node] = th;
+      if (do_theta) th_out[node] = s[4];
     }
-    i += W;
+    i += P;
     if (i >= n) break;
     rec = rec_next;
     rec_next = rec_nn;
-    ka = ka_n;
-    kb = kb_n;
+    k_cur = k_next;
   }
 }
 
@@ -638,7 +633,7 @@ cudaError_t dense_prepare(DenseGeo &dg, const Abc &ab) {
   int per_sm = 0;
   cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_abc_pipe, 256, 0);
   if (e != cudaSuccess) return e;
-  const int need = (ab.n_recs + kAbcWarpsPerBlock - 1) / kAbcWarpsPerBlock;
+  const int need = (ab.n_recs + kAbcWarpsPerBlock / 2 - 1) / (kAbcWarpsPerBlock / 2);
   dg.abc_grid = std::max(1, std::min(need, std::max(per_sm, 1) * n_sm));
   return cudaSuccess;
 }
