@@ -280,6 +280,61 @@ int upload_abc(lps_handle *h, const HostAbc &H, int total_abc, const std::vector
   return LPS_OK;
 }
 
+// Dense path: the sliced-ELL copy of the operators (see Abc::sell_g).
+int upload_abc_sell(lps_handle *h, const HostAbc &H) {
+  Abc &B = h->lg.abc;
+  std::vector<int> ents;
+  for (size_t a = 0; a < H.writes.size(); a++)
+    if (H.writes[a]) ents.push_back((int)a);
+  // longest clouds first; equal lengths keep their order (neighbouring
+  // entries share cloud nodes)
+  std::stable_sort(ents.begin(), ents.end(), [&](int x, int y) { return H.cl_len[x] > H.cl_len[y]; });
+  const int n_sl = ((int)ents.size() + 31) / 32;
+  std::vector<SellSlice> sl(n_sl);
+  std::vector<double> g;
+  std::vector<int> ix, sa((size_t)n_sl * 32, -1);
+  for (int s = 0; s < n_sl; s++) {
+    int len = 1;
+    for (int l = 0; l < 32 && 32 * s + l < (int)ents.size(); l++) len = std::max(len, H.cl_len[ents[32 * s + l]]);
+    sl[s].goff = (long long)g.size();
+    sl[s].ioff = (long long)ix.size();
+    sl[s].len = len;
+    sl[s].pad = 0;
+    const int fill_node = H.node[ents[32 * s]];
+    g.resize(g.size() + (size_t)len * 18 * 32, 0.0);
+    ix.resize(ix.size() + (size_t)len * 32, fill_node);
+    double *gs = g.data() + sl[s].goff;
+    int *is = ix.data() + sl[s].ioff;
+    for (int l = 0; l < 32 && 32 * s + l < (int)ents.size(); l++) {
+      const int a = ents[32 * s + l];
+      sa[(size_t)32 * s + l] = a;
+      const size_t o = H.cl_off[a];
+      const int la = H.cl_len[a];
+      for (int e = 0; e < la; e++) {
+        is[(size_t)e * 32 + l] = H.cl_idx[o + e];
+        for (int r = 0; r < 8; r++) {
+          gs[((size_t)e * 18 + r) * 32 + l] = H.gu[8 * o + (size_t)r * la + e];
+          gs[((size_t)e * 18 + 8 + r) * 32 + l] = H.gv[8 * o + (size_t)r * la + e];
+        }
+        for (int r = 0; r < 2; r++) gs[((size_t)e * 18 + 16 + r) * 32 + l] = H.gth[2 * o + (size_t)r * la + e];
+      }
+    }
+  }
+  SellSlice *d_sl;
+  double *d_g;
+  int *d_ix, *d_sa;
+  int s;
+  if ((s = dev_upload(h, &d_sl, sl)) || (s = dev_upload(h, &d_g, g)) || (s = dev_upload(h, &d_ix, ix)) ||
+      (s = dev_upload(h, &d_sa, sa)))
+    return s;
+  B.n_slices = n_sl;
+  B.slices = d_sl;
+  B.sell_g = d_g;
+  B.sell_idx = d_ix;
+  B.sell_a = d_sa;
+  return LPS_OK;
+}
+
 // ---------------------------------------------------------------------------
 int build_csr(lps_handle *h, const lps_problem *probs) {
   const int K = h->n_inst;
@@ -609,6 +664,7 @@ int build_dense(lps_handle *h, const lps_problem *probs, const std::vector<Latti
   D.fp32 = h->opt.precision == LPS_FP32_MIXED;
   if (D.fp32 && (st = dev_upload(h, &h->coef32, coef32))) return st;
   if ((st = upload_abc(h, H, total_abc, abc_of))) return st;
+  if ((st = upload_abc_sell(h, H))) return st;
   std::map<int, int> done;
   for (int k = 0; k < K; k++) {
     if (done.count(lat[k].M)) continue;

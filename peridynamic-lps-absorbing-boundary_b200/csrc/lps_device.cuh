@@ -110,7 +110,23 @@ struct Abc {
   // (cloud offset, cloud length, node, entry | instance << 24).
   const int4 *recs;
   int n_recs;
-  int pad_;
+  // Dense path, sliced-ELL copy of the operators: the writing entries sorted
+  // by cloud length and cut into slices of 32 (one entry per lane); slice s
+  // holds for each cloud position e < len_s the 18 operator rows of its 32
+  // entries ([e][row][lane], doubles) and their cloud indices ([e][lane]),
+  // zero weights (and a valid index) past an entry's own length.
+  int n_slices;
+  const struct SellSlice *slices;
+  const double *sell_g;
+  const int *sell_idx;
+  const int *sell_a;           // [slice][lane]: ABC entry, or -1
+};
+
+struct SellSlice {
+  long long goff;              // first double of the slice in sell_g
+  long long ioff;              // first int of the slice in sell_idx
+  int len;                     // cloud positions in the slice
+  int pad;
 };
 
 // Per-block partial sums of the diagnostics (src/main.cpp:986-1062).

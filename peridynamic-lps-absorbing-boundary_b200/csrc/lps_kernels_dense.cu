@@ -437,6 +437,72 @@ __global__ void __launch_bounds__(256, 3) k_abc_pipe(Abc ab, StepPtrs p, int do_
   }
 }
 
+// The absorbing boundary of a dense step over the sliced-ELL operators: one
+// CTA per slice of 32 writing entries (one per lane), kSellWarps warps that
+// split the slice's cloud positions; a warp's operator reads are 256-byte
+// rows of one contiguous run, so the operator stream reaches DRAM in long
+// sequential pieces.  Per entry: G_u and G_v of this step (src/main.cpp:
+// 883-916, :933-974) from u^n, u^{n-1}, v^n, v^{n-1}, and, one step ahead,
+// G_theta (:792-812): theta^{n+2} from theta^{n+1} (p.th_np1) and theta^n
+// (p.th_n) into the ring slot that theta^{n-1} (p.th_nm1) frees.  Warps add
+// their partial sums through shared memory.
+constexpr int kSellWarps = 4;
+
+__global__ void __launch_bounds__(32 * kSellWarps) k_abc_sell(Abc ab, StepPtrs p, int do_uv, int do_theta) {
+  __shared__ double red[kSellWarps - 1][5][32];
+  const int lane = threadIdx.x & 31, q = threadIdx.x >> 5;
+  const SellSlice sl = ab.slices[blockIdx.x];
+  const int a = ab.sell_a[blockIdx.x * 32 + lane];
+  const int inst = a >= 0 ? ab.inst[a] : 0;
+  const bool kin = c_inst[inst].kinematic != 0;
+  const int e0 = q * sl.len / kSellWarps, e1 = (q + 1) * sl.len / kSellWarps;
+  const double *__restrict__ g = ab.sell_g + sl.goff + lane;
+  const int *__restrict__ ix = ab.sell_idx + sl.ioff + lane;
+  double s[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // ux, uy, vx, vy, theta
+#pragma unroll 2
+  for (int e = e0; e < e1; e++) {
+    const int k = __ldg(ix + 32 * e);
+    const double *__restrict__ ge = g + (size_t)e * 18 * 32;
+    if (do_uv) {
+      const double2 un = p.u_n[k], um = p.u_nm1[k];
+      s[0] += __ldcs(ge + 0 * 32) * un.x + __ldcs(ge + 1 * 32) * un.y + __ldcs(ge + 2 * 32) * um.x +
+              __ldcs(ge + 3 * 32) * um.y;
+      s[1] += __ldcs(ge + 4 * 32) * un.x + __ldcs(ge + 5 * 32) * un.y + __ldcs(ge + 6 * 32) * um.x +
+              __ldcs(ge + 7 * 32) * um.y;
+      if (!kin) {
+        const double2 vn = p.v_n[k], vm = p.v_nm1[k];
+        s[2] += __ldcs(ge + 8 * 32) * vn.x + __ldcs(ge + 9 * 32) * vn.y + __ldcs(ge + 10 * 32) * vm.x +
+                __ldcs(ge + 11 * 32) * vm.y;
+        s[3] += __ldcs(ge + 12 * 32) * vn.x + __ldcs(ge + 13 * 32) * vn.y + __ldcs(ge + 14 * 32) * vm.x +
+                __ldcs(ge + 15 * 32) * vm.y;
+      }
+    }
+    if (do_theta) s[4] += __ldcs(ge + 16 * 32) * p.th_np1[k] + __ldcs(ge + 17 * 32) * p.th_n[k];
+  }
+  if (q > 0)
+#pragma unroll
+    for (int j = 0; j < 5; j++) red[q - 1][j][lane] = s[j];
+  __syncthreads();
+  if (q > 0 || a < 0) return;
+#pragma unroll
+  for (int w = 0; w < kSellWarps - 1; w++)
+#pragma unroll
+    for (int j = 0; j < 5; j++) s[j] += red[w][j][lane];
+  const int node = ab.node[a];
+  if (do_uv) {
+    p.s_abc[a] = make_double2(s[0], s[1]);
+    if (kin) {
+      // v = (u^{n+1} - u^n) / dt with this node's u^n, src/main.cpp:940-943
+      const double2 un = p.u_n[node];
+      const double dt = c_inst[inst].dt;
+      p.v_np1[node] = make_double2((s[0] - un.x) / dt, (s[1] - un.y) / dt);
+    } else {
+      p.v_np1[node] = make_double2(s[2], s[3]);
+    }
+  }
+  if (do_theta) const_cast<double *>(p.th_nm1)[node] = s[4];
+}
+
 // End of a dense step at the absorbing boundary, after the force tiles and
 // G_u/G_v: this step's G_u result u^{n+1} goes into the displacement ring,
 // and u^{n+2} is predicted there from it, the G_v velocity and the new
@@ -760,8 +826,8 @@ int enqueue_dense_step(const DenseGeo &dg, const LaunchGeo &lg, const StepPtrs &
       cudaEventRecord(dg.ev_fork[0], st);
       cudaStreamWaitEvent(side, dg.ev_fork[0], 0);
     }
-    k_abc_pipe<<<dg.abc_grid, 256, 0, side>>>(lg.abc, p, 1, gth ? 1 : 0);
-    if (mark) (*mark)("abc_pipe");
+    k_abc_sell<<<lg.abc.n_slices, 32 * kSellWarps, 0, side>>>(lg.abc, p, 1, gth ? 1 : 0);
+    if (mark) (*mark)("abc_sell");
     k++;
     if (fork) cudaEventRecord(dg.ev_join[1], side);
   }
@@ -797,7 +863,7 @@ void launch_abc_theta_dense(const DenseGeo &dg, const LaunchGeo &lg, const doubl
   p.th_np1 = const_cast<double *>(th_n);  // the kernel's "newer" level
   p.th_n = th_nm1;
   p.th_nm1 = th_np1;                       // output slot
-  k_abc_pipe<<<dg.abc_grid, 256, 0, st>>>(lg.abc, p, 0, 1);
+  k_abc_sell<<<lg.abc.n_slices, 32 * kSellWarps, 0, st>>>(lg.abc, p, 0, 1);
 }
 
 void launch_theta_dense_init(const DenseGeo &, const LaunchGeo &lg, const double2 *u, double *theta,
