@@ -300,9 +300,8 @@ int upload_abc_sell(lps_handle *h, const HostAbc &H) {
     sl[s].ioff = (long long)ix.size();
     sl[s].len = len;
     sl[s].pad = 0;
-    const int fill_node = H.node[ents[32 * s]];
     g.resize(g.size() + (size_t)len * 18 * 32, 0.0);
-    ix.resize(ix.size() + (size_t)len * 32, fill_node);
+    ix.resize(ix.size() + (size_t)len * 32, H.node[ents[32 * s]]);
     double *gs = g.data() + sl[s].goff;
     int *is = ix.data() + sl[s].ioff;
     for (int l = 0; l < 32 && 32 * s + l < (int)ents.size(); l++) {
@@ -310,6 +309,9 @@ int upload_abc_sell(lps_handle *h, const HostAbc &H) {
       sa[(size_t)32 * s + l] = a;
       const size_t o = H.cl_off[a];
       const int la = H.cl_len[a];
+      // past its own cloud a lane reads its own node with zero weights, so a
+      // NaN in another instance of the slice cannot reach it
+      for (int e = la; e < len; e++) is[(size_t)e * 32 + l] = H.node[a];
       for (int e = 0; e < la; e++) {
         is[(size_t)e * 32 + l] = H.cl_idx[o + e];
         for (int r = 0; r < 8; r++) {

@@ -455,12 +455,14 @@ __global__ void __launch_bounds__(32 * kSellWarps) k_abc_sell(Abc ab, StepPtrs p
   const int a = ab.sell_a[blockIdx.x * 32 + lane];
   const int inst = a >= 0 ? ab.inst[a] : 0;
   const bool kin = c_inst[inst].kinematic != 0;
-  const int e0 = q * sl.len / kSellWarps, e1 = (q + 1) * sl.len / kSellWarps;
   const double *__restrict__ g = ab.sell_g + sl.goff + lane;
   const int *__restrict__ ix = ab.sell_idx + sl.ioff + lane;
   double s[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // ux, uy, vx, vy, theta
+  // warp q takes positions q, q + 4, ...: which warp sums a position does
+  // not depend on the slice's length, so an entry's result does not depend on
+  // the entries it shares a slice with (past its own length it adds zeros)
 #pragma unroll 2
-  for (int e = e0; e < e1; e++) {
+  for (int e = q; e < sl.len; e += kSellWarps) {
     const int k = __ldg(ix + 32 * e);
     const double *__restrict__ ge = g + (size_t)e * 18 * 32;
     if (do_uv) {
