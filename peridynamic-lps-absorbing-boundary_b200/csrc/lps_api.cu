@@ -259,20 +259,6 @@ int upload_abc(lps_handle *h, const HostAbc &H, int total_abc, const std::vector
       (s = dev_upload(h, &a_gu, H.gu)) || (s = dev_upload(h, &a_gv, H.gv)) ||
       (s = dev_upload(h, &a_idw_w, H.idw_w)) || (s = dev_upload(h, &a_gth, H.gth)))
     return s;
-  // records of the writing entries (dense pipelined kernel; harmless for CSR)
-  if (total_abc >= (1 << 24)) {
-    h->err = "more than 2^24 absorbing-boundary entries in one batch";
-    return LPS_ERR_UNSUPPORTED;
-  }
-  {
-    std::vector<int4> recs;
-    for (int a = 0; a < total_abc; a++)
-      if (H.writes[a]) recs.push_back(make_int4(H.cl_off[a], H.cl_len[a], H.node[a], a | (H.inst[a] << 24)));
-    int4 *d_recs;
-    if ((s = dev_upload(h, &d_recs, recs))) return s;
-    B.recs = d_recs;
-    B.n_recs = (int)recs.size();
-  }
   B.n_abc = total_abc;
   B.node = a_node; B.inst = a_inst; B.cl_off = a_cl_off; B.cl_len = a_cl_len; B.cl_idx = a_cl_idx;
   B.idw_off = a_idw_off; B.idw_len = a_idw_len; B.idw_idx = a_idw_idx; B.writes = a_writes;
@@ -673,7 +659,7 @@ int build_dense(lps_handle *h, const lps_problem *probs, const std::vector<Latti
     done[lat[k].M] = 1;
     LPS_CUDA_TRY(h, upload_dense_constants(lat[k].M, probs[k].dx, probs[k].dy, probs[k].delta, h->stream));
   }
-  LPS_CUDA_TRY(h, dense_prepare(D, h->lg.abc));
+  LPS_CUDA_TRY(h, dense_prepare(D));
   h->lg.n_node_blocks = n / kNodeBlock;
   h->lg.n_abc_blocks = total_abc / kAbcWarpsPerBlock;
   h->lg.n_inst = K;

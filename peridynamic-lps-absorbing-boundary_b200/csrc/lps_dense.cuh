@@ -70,7 +70,6 @@ struct DenseGeo {
   int total_rows = 0;
   int tile_priority = 0;                       // launch priority of the tile kernels
   bool fp32 = false;                           // FP32-mixed tile kernels
-  int abc_grid = 0;                            // persistent grid of the pipelined ABC kernel
   cudaStream_t side = nullptr;                 // forked stream for the ABC kernels
   cudaEvent_t ev_fork[2] = {nullptr, nullptr}, ev_join[2] = {nullptr, nullptr};
   int *d_err = nullptr;                        // device wait-timeout flag
@@ -96,9 +95,8 @@ cudaError_t upload_dense_constants(int m, double dx, double dy, double delta, cu
 int dense_encode_maps(DenseGroup &g, int pitch, int total_rows, double2 *const *U, double *const *TH,
                       const double2 *coef, const uint8_t *type, float2 *const *U32, const float2 *coef32,
                       std::string &err);
-// Sets shared-memory limits and the persistent grid sizes of each group and
-// of the pipelined absorbing-boundary kernel.
-cudaError_t dense_prepare(DenseGeo &dg, const Abc &ab);
+// Sets shared-memory limits and the persistent grid sizes of each group.
+cudaError_t dense_prepare(DenseGeo &dg);
 
 // FP32-mixed tile kernels (lps_kernels_dense32.cu): shared-memory limits,
 // persistent grids and launches of one group.

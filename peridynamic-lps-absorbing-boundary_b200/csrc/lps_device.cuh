@@ -106,10 +106,6 @@ struct Abc {
   const int *idw_off, *idw_len;// IDW neighbour lists (THETA_ABC_METHOD 0)
   const int *idw_idx;
   const double *idw_w;
-  // Dense path: one record per writing entry for the pipelined kernel --
-  // (cloud offset, cloud length, node, entry | instance << 24).
-  const int4 *recs;
-  int n_recs;
   // Dense path, sliced-ELL copy of the operators: the writing entries sorted
   // by cloud length and cut into slices of 32 (one entry per lane); slice s
   // holds for each cloud position e < len_s the 18 operator rows of its 32

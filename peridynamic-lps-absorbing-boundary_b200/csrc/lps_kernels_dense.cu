@@ -6,7 +6,7 @@
 //                    displacements
 //   k_force_tma<M>   force (:821-874), corrector (:922-925) and the next
 //                    step's predictor (:725-728)
-//   k_abc_pipe       G_u, G_v (:883-916, :933-974) of the step and G_theta
+//   k_abc_sell       G_u, G_v (:883-916, :933-974) of the step and G_theta
 //                    (:792-812) of the next, on a side stream beside the force
 //                    tiles
 //   k_abc_predict    the ABC nodes' merge and prediction at the end of the step
@@ -350,93 +350,6 @@ __global__ void __launch_bounds__(kTileThreads, 2)
 
 // ---------------------------------------------------------------------------
 // Absorbing-boundary kernels of the dense path.
-// One cloud entry's contribution to the x and y outputs of a 2-level operator
-// (rows component-major, len doubles each), with streaming loads: the
-// operators are read once per step, so they should not push the gathered
-// state out of L2.
-__device__ __forceinline__ void g_entry_stream(const double *__restrict__ g, int len, int e, double2 xn, double2 xm,
-                                               double &ox, double &oy) {
-  ox += __ldcs(g + 0 * len + e) * xn.x + __ldcs(g + 1 * len + e) * xn.y + __ldcs(g + 2 * len + e) * xm.x +
-        __ldcs(g + 3 * len + e) * xm.y;
-  oy += __ldcs(g + 4 * len + e) * xn.x + __ldcs(g + 5 * len + e) * xn.y + __ldcs(g + 6 * len + e) * xm.x +
-        __ldcs(g + 7 * len + e) * xm.y;
-}
-
-// The absorbing boundary of a dense step, software-pipelined over a warp
-// pair per entry: a persistent pair of warps walks the writing entries
-// i, i + P, ... (P pairs in the grid); each warp takes every other 32 cloud
-// entries of an entry, one per lane, so a lane keeps the operator rows and the
-// gathered state of a single cloud entry in flight at once, and it loads the
-// record of entry i + 2P and its cloud indices of entry i + P while it works
-// on entry i.  The odd warp hands its partial sums to the even one through
-// shared memory (a 64-thread named barrier per pair).  Per entry: G_u and G_v
-// of this step (src/main.cpp:883-916, :933-974) from u^n, u^{n-1}, v^n,
-// v^{n-1}, and, one step ahead, G_theta (:792-812): theta^{n+2} from
-// theta^{n+1} (p.th_np1) and theta^n (p.th_n) into the ring slot that
-// theta^{n-1} (p.th_nm1) frees.
-__global__ void __launch_bounds__(256, 3) k_abc_pipe(Abc ab, StepPtrs p, int do_uv, int do_theta) {
-  __shared__ double part[2][kAbcWarpsPerBlock / 2][5];
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, half = wib & 1, pib = wib >> 1;
-  const int P = gridDim.x * (kAbcWarpsPerBlock / 2);
-  const int n = ab.n_recs;
-  int i = blockIdx.x * (kAbcWarpsPerBlock / 2) + pib;
-  if (i >= n) return;  // both warps of the pair leave together
-  double *th_out = const_cast<double *>(p.th_nm1);
-  const int4 z4 = make_int4(0, 0, 0, 0);
-  const int e_first = 32 * half + lane;  // this lane's first cloud entry; then every 64
-  int4 rec = ab.recs[i];
-  int4 rec_next = i + P < n ? ab.recs[i + P] : z4;
-  int k_cur = e_first < rec.y ? __ldg(ab.cl_idx + rec.x + e_first) : 0;
-  for (int it = 0;; it++) {
-    // prefetch: this lane's first cloud index of the next entry, record of the one after
-    const int k_next = e_first < rec_next.y ? __ldg(ab.cl_idx + rec_next.x + e_first) : 0;
-    const int4 rec_nn = i + 2 * P < n ? ab.recs[i + 2 * P] : z4;
-    const int off = rec.x, len = rec.y, node = rec.z, a = rec.w & 0xffffff;
-    const InstParams &Pi = c_inst[rec.w >> 24];
-    const bool kin = Pi.kinematic != 0;
-    const double *__restrict__ gu = ab.gu + 8 * (size_t)off;
-    const double *__restrict__ gv = ab.gv + 8 * (size_t)off;
-    const double *__restrict__ w0 = ab.gth + 2 * (size_t)off;
-    const double *__restrict__ w1 = w0 + len;
-    double s[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // ux, uy, vx, vy, theta
-    for (int e = e_first; e < len; e += 64) {
-      const int k = e == e_first ? k_cur : __ldg(ab.cl_idx + off + e);
-      if (do_uv) {
-        g_entry_stream(gu, len, e, p.u_n[k], p.u_nm1[k], s[0], s[1]);
-        if (!kin) g_entry_stream(gv, len, e, p.v_n[k], p.v_nm1[k], s[2], s[3]);
-      }
-      if (do_theta) s[4] += __ldcs(w0 + e) * p.th_np1[k] + __ldcs(w1 + e) * p.th_n[k];
-    }
-#pragma unroll
-    for (int j = 0; j < 5; j++) s[j] = warp_sum(s[j]);
-    double(*buf)[5] = part[it & 1];
-    if (half == 1 && lane == 0)
-#pragma unroll
-      for (int j = 0; j < 5; j++) buf[pib][j] = s[j];
-    asm volatile("bar.sync %0, 64;" ::"r"(1 + pib) : "memory");
-    if (half == 0 && lane == 0) {
-#pragma unroll
-      for (int j = 0; j < 5; j++) s[j] += buf[pib][j];
-      if (do_uv) {
-        p.s_abc[a] = make_double2(s[0], s[1]);
-        if (kin) {
-          // v = (u^{n+1} - u^n) / dt with this node's u^n, src/main.cpp:940-943
-          const double2 un = p.u_n[node];
-          p.v_np1[node] = make_double2((s[0] - un.x) / Pi.dt, (s[1] - un.y) / Pi.dt);
-        } else {
-          p.v_np1[node] = make_double2(s[2], s[3]);
-        }
-      }
-      if (do_theta) th_out[node] = s[4];
-    }
-    i += P;
-    if (i >= n) break;
-    rec = rec_next;
-    rec_next = rec_nn;
-    k_cur = k_next;
-  }
-}
-
 // The absorbing boundary of a dense step over the sliced-ELL operators: one
 // CTA per slice of 32 writing entries (one per lane), kSellWarps warps that
 // split the slice's cloud positions; a warp's operator reads are 256-byte
@@ -446,7 +359,7 @@ __global__ void __launch_bounds__(256, 3) k_abc_pipe(Abc ab, StepPtrs p, int do_
 // G_theta (:792-812): theta^{n+2} from theta^{n+1} (p.th_np1) and theta^n
 // (p.th_n) into the ring slot that theta^{n-1} (p.th_nm1) frees.  Warps add
 // their partial sums through shared memory.
-constexpr int kSellWarps = 4;
+constexpr int kSellWarps = 4;  // 2: 70.0 us, 4: 68.3 us, 8: 65.9 us standalone; the same step time
 
 __global__ void __launch_bounds__(32 * kSellWarps) k_abc_sell(Abc ab, StepPtrs p, int do_uv, int do_theta) {
   __shared__ double red[kSellWarps - 1][5][32];
@@ -684,7 +597,7 @@ static void prepare_dispatch(DenseGroup &gr, int n_sm, cudaError_t *e) {
   *e = prepare_m<M>(gr, n_sm);
 }
 
-cudaError_t dense_prepare(DenseGeo &dg, const Abc &ab) {
+cudaError_t dense_prepare(DenseGeo &dg) {
   int dev = 0, n_sm = 0, least = 0, greatest = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
@@ -698,11 +611,6 @@ cudaError_t dense_prepare(DenseGeo &dg, const Abc &ab) {
       LPS_DISPATCH_M(gr.m, prepare_dispatch, gr, n_sm, &e);
     if (e != cudaSuccess) return e;
   }
-  int per_sm = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_abc_pipe, 256, 0);
-  if (e != cudaSuccess) return e;
-  const int need = (ab.n_recs + kAbcWarpsPerBlock / 2 - 1) / (kAbcWarpsPerBlock / 2);
-  dg.abc_grid = std::max(1, std::min(need, std::max(per_sm, 1) * n_sm));
   return cudaSuccess;
 }
 
@@ -803,7 +711,7 @@ int enqueue_dense_step(const DenseGeo &dg, const LaunchGeo &lg, const StepPtrs &
   // (serialised), so each kernel's device time can be read between events.
   const bool fork = mark == nullptr;
   cudaStream_t side = fork ? dg.side : st;
-  // The absorbing boundary is one pipelined kernel after the dilatation
+  // The absorbing boundary is one kernel after the dilatation
   // tiles: G_u/G_v of this step and G_theta of the next (theta^{n+2} at ABC
   // nodes from theta^{n+1}, theta^n, into the ring slot theta^{n-1} frees;
   // the reset computes the first one).  It runs on the side stream beside the
@@ -822,7 +730,7 @@ int enqueue_dense_step(const DenseGeo &dg, const LaunchGeo &lg, const StepPtrs &
     if (mark) (*mark)("theta_idw");
     k++;
   }
-  const bool pipe = abc && lg.abc.n_recs > 0;
+  const bool pipe = abc && lg.abc.n_slices > 0;
   if (pipe) {
     if (fork) {
       cudaEventRecord(dg.ev_fork[0], st);
@@ -860,7 +768,7 @@ void launch_dense_reset_predict(const LaunchGeo &lg, const double2 *u0, const do
 
 void launch_abc_theta_dense(const DenseGeo &dg, const LaunchGeo &lg, const double *th_n, const double *th_nm1,
                             double *th_np1, cudaStream_t st) {
-  if (lg.abc.n_recs == 0) return;
+  if (lg.abc.n_slices == 0) return;
   StepPtrs p = {};
   p.th_np1 = const_cast<double *>(th_n);  // the kernel's "newer" level
   p.th_n = th_nm1;
