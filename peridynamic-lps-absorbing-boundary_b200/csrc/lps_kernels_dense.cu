@@ -446,18 +446,18 @@ __global__ void __launch_bounds__(256) k_abc_predict(Abc ab, StepPtrs p) {
 // energy/momentum partial sums (:986-1062).
 template <int M>
 __device__ __forceinline__ double theta_cell(const Geo &g, const double2 *u, size_t cell, int pitch) {
-  constexpr Sten<M> S = make_sten<M>();
   const double2 ui = u[cell];
   double s0 = 0.0, s1 = 0.0;
-#pragma unroll
-  for (int j = 0; j < Sten<M>::N; j++) {
-    const size_t nb = cell + (ptrdiff_t)S.a[j] * pitch + S.b[j];
+  static_for<0, Sten<M>::N>([&](auto jc) {
+    constexpr int j = decltype(jc)::value;
+    constexpr int a = make_sten<M>().a[j], b = make_sten<M>().b[j];
+    const size_t nb = cell + (ptrdiff_t)a * pitch + b;
     if (g.type[nb] & kExists) {
       const double2 uj = u[nb];
       s0 = fma(SC<M>(5, j), uj.x - ui.x, s0);
       s1 = fma(SC<M>(6, j), uj.y - ui.y, s1);
     }
-  }
+  });
   const double mi = g.m[cell];
   return (mi > 0.0) ? (2.0 / mi) * (s0 + s1) : 0.0;
 }
@@ -480,12 +480,12 @@ __global__ void __launch_bounds__(256) k_theta_dense_init(Geo g, const double2 *
 template <int M>
 __device__ __forceinline__ void wdev_cell(const Geo &g, const double2 *u, size_t cell, int pitch, double th,
                                           double coef, double *W) {
-  constexpr Sten<M> S = make_sten<M>();
   const double2 ui = u[cell];
   double w = 0.0;
-#pragma unroll
-  for (int j = 0; j < Sten<M>::N; j++) {
-    const size_t nb = cell + (ptrdiff_t)S.a[j] * pitch + S.b[j];
+  static_for<0, Sten<M>::N>([&](auto jc) {
+    constexpr int j = decltype(jc)::value;
+    constexpr int a = make_sten<M>().a[j], b = make_sten<M>().b[j];
+    const size_t nb = cell + (ptrdiff_t)a * pitch + b;
     if (g.type[nb] & kExists) {
       const double2 uj = u[nb];
       const double e = SC<M>(0, j) * (uj.x - ui.x) + SC<M>(1, j) * (uj.y - ui.y);
@@ -493,7 +493,7 @@ __device__ __forceinline__ void wdev_cell(const Geo &g, const double2 *u, size_t
       const double bdv = SC<M>(3, j) * SC<M>(0, j) + SC<M>(4, j) * SC<M>(1, j);
       w += coef * ed * ed * bdv;
     }
-  }
+  });
   *W = w;
 }
 

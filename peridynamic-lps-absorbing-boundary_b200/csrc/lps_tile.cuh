@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <type_traits>
+#include <utility>
 
 #include "lps_dense.cuh"
 
@@ -54,12 +55,13 @@ __host__ __device__ constexpr int amax(int M, int b) {
 // Compile-time loop: f(std::integral_constant<int, I>) for I in [I0, N), so
 // that stencil offsets, table indices and per-offset constants inside f are
 // constant expressions (not values the optimiser may or may not fold).
-template <int I, int N, class F>
+template <int I0, class F, int... Is>
+__device__ __forceinline__ void static_for_seq(F &&f, std::integer_sequence<int, Is...>) {
+  (f(std::integral_constant<int, I0 + Is>{}), ...);  // in order, no recursion depth
+}
+template <int I0, int N, class F>
 __device__ __forceinline__ void static_for(F &&f) {
-  if constexpr (I < N) {
-    f(std::integral_constant<int, I>{});
-    static_for<I + 1, N>(f);
-  }
+  if constexpr (N > I0) static_for_seq<I0>(f, std::make_integer_sequence<int, N - I0>{});
 }
 
 // Visits the offset pairs (a, b) / (-a, -b) of ratio M column by column,
