@@ -451,7 +451,7 @@ __device__ __forceinline__ double theta_cell(const Geo &g, const double2 *u, siz
   static_for<0, Sten<M>::N>([&](auto jc) {
     constexpr int j = decltype(jc)::value;
     constexpr int a = make_sten<M>().a[j], b = make_sten<M>().b[j];
-    const size_t nb = cell + (ptrdiff_t)a * pitch + b;
+    const size_t nb = (size_t)((ptrdiff_t)cell + (ptrdiff_t)a * pitch + b);
     if (g.type[nb] & kExists) {
       const double2 uj = u[nb];
       s0 = fma(SC<M>(5, j), uj.x - ui.x, s0);
@@ -485,7 +485,7 @@ __device__ __forceinline__ void wdev_cell(const Geo &g, const double2 *u, size_t
   static_for<0, Sten<M>::N>([&](auto jc) {
     constexpr int j = decltype(jc)::value;
     constexpr int a = make_sten<M>().a[j], b = make_sten<M>().b[j];
-    const size_t nb = cell + (ptrdiff_t)a * pitch + b;
+    const size_t nb = (size_t)((ptrdiff_t)cell + (ptrdiff_t)a * pitch + b);
     if (g.type[nb] & kExists) {
       const double2 uj = u[nb];
       const double e = SC<M>(0, j) * (uj.x - ui.x) + SC<M>(1, j) * (uj.y - ui.y);
