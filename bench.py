@@ -207,10 +207,9 @@ def algorithmic_bytes(sets, kernel, precision="fp64"):
         "force_tiles": ((128 if f32 else 120) * n, (56 if f32 else 80) * n),
         # dilatation: read u_pred 16 (FP32-mixed: 8), m 8; write theta 8
         "theta_tiles": ((24 if f32 else 32) * n, None),
-        # G_u, G_v: 2 x 8C doubles + 4C index bytes per ABC node
-        "abc_uv": (132 * abc, None),
-        # G_theta: 2C doubles + 4C index bytes per ABC node
-        "abc_theta": (20 * abc, None),
+        # G_u, G_v of the step and G_theta of the next: 18C doubles + 4C index
+        # bytes per ABC node (the gathered state hits L2)
+        "abc_sell": (148 * abc, 148 * abc),
         # neighbour-list path
         "predict_csr": (80 * n, None),
         "theta_csr": (32 * n, None),
@@ -223,13 +222,13 @@ def algorithmic_bytes(sets, kernel, precision="fp64"):
     return table.get(kernel, (None, None))
 
 
-def measured_traffic(kernel):
-    """DRAM bytes per launch from the committed ncu summary, if listed."""
+def measured_traffic(kernel, precision):
+    """DRAM bytes per launch from the committed ncu summaries, if listed."""
     p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if not os.path.exists(p):
         return None
     d = json.load(open(p))
-    return d.get("kernels", {}).get(kernel, {}).get("dram_bytes_per_launch")
+    return d.get(precision, {}).get(kernel, {}).get("dram_bytes_per_launch")
 
 
 # ---------------------------------------------------------------------------
@@ -329,11 +328,11 @@ def run_ours(args, rank, world, local_rank, precision, with_cpu=True):
     for k, v in prof.items():
         b, _ = algorithmic_bytes(sets, k, precision)
         kernels[k] = {"launches": v[0], "ms_per_launch": v[1] / v[0], "algorithmic_bytes": b,
-                      "achieved_gbs": gbs(b, v[1] / v[0]), "traffic": measured_traffic(k)}
+                      "achieved_gbs": gbs(b, v[1] / v[0]), "traffic": measured_traffic(k, precision)}
     step_bytes, _ = algorithmic_bytes(sets, "step", precision)
     roofline = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
-                "traffic": measured_traffic(name), "algorithmic_bytes_per_launch": ab_grade or ab,
+                "traffic": measured_traffic(name, precision), "algorithmic_bytes_per_launch": ab_grade or ab,
                 "actual_layout_bytes_per_launch": ab, "ms_per_launch": per_launch_ms,
                 "kernels": kernels, "serialized_step_ms": step_ms,
                 "step_algorithmic_bytes": step_bytes,
