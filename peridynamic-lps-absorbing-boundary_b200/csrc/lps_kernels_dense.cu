@@ -359,10 +359,14 @@ __global__ void __launch_bounds__(kTileThreads, 2)
 // G_theta (:792-812): theta^{n+2} from theta^{n+1} (p.th_np1) and theta^n
 // (p.th_n) into the ring slot that theta^{n-1} (p.th_nm1) frees.  Warps add
 // their partial sums through shared memory.
-constexpr int kSellWarps = 4;  // 2: 70.0 us, 4: 68.3 us, 8: 65.9 us standalone; the same step time
+// Measured (7-instance batch, standalone): 4 warps 68.3 us without and
+// 60.7 us with the cloud index loaded one position ahead; 8 warps 63.6 us;
+// 4 or 8 warps at 46 registers 67.1 / 60.5 us.
+constexpr int kSellWarps = 4;
 
 __global__ void __launch_bounds__(32 * kSellWarps) k_abc_sell(Abc ab, StepPtrs p, int do_uv, int do_theta) {
-  __shared__ double red[kSellWarps - 1][5][32];
+  constexpr int W = kSellWarps;
+  __shared__ double red[W - 1][5][32];
   const int lane = threadIdx.x & 31, q = threadIdx.x >> 5;
   const SellSlice sl = ab.slices[blockIdx.x];
   const int a = ab.sell_a[blockIdx.x * 32 + lane];
@@ -371,12 +375,14 @@ __global__ void __launch_bounds__(32 * kSellWarps) k_abc_sell(Abc ab, StepPtrs p
   const double *__restrict__ g = ab.sell_g + sl.goff + lane;
   const int *__restrict__ ix = ab.sell_idx + sl.ioff + lane;
   double s[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // ux, uy, vx, vy, theta
-  // warp q takes positions q, q + 4, ...: which warp sums a position does
+  // warp q takes positions q, q + W, ...: which warp sums a position does
   // not depend on the slice's length, so an entry's result does not depend on
   // the entries it shares a slice with (past its own length it adds zeros)
+  int k_next = q < sl.len ? __ldg(ix + 32 * q) : 0;
 #pragma unroll 2
-  for (int e = q; e < sl.len; e += kSellWarps) {
-    const int k = __ldg(ix + 32 * e);
+  for (int e = q; e < sl.len; e += W) {
+    const int k = k_next;  // this position's cloud index, loaded one position ahead
+    if (e + W < sl.len) k_next = __ldg(ix + 32 * (e + W));
     const double *__restrict__ ge = g + (size_t)e * 18 * 32;
     if (do_uv) {
       const double2 un = p.u_n[k], um = p.u_nm1[k];
@@ -400,7 +406,7 @@ __global__ void __launch_bounds__(32 * kSellWarps) k_abc_sell(Abc ab, StepPtrs p
   __syncthreads();
   if (q > 0 || a < 0) return;
 #pragma unroll
-  for (int w = 0; w < kSellWarps - 1; w++)
+  for (int w = 0; w < W - 1; w++)
 #pragma unroll
     for (int j = 0; j < 5; j++) s[j] += red[w][j][lane];
   const int node = ab.node[a];
@@ -416,6 +422,10 @@ __global__ void __launch_bounds__(32 * kSellWarps) k_abc_sell(Abc ab, StepPtrs p
     }
   }
   if (do_theta) const_cast<double *>(p.th_nm1)[node] = s[4];
+}
+
+static void launch_abc_sell(const Abc &ab, const StepPtrs &p, int do_uv, int do_theta, cudaStream_t st) {
+  k_abc_sell<<<ab.n_slices, 32 * kSellWarps, 0, st>>>(ab, p, do_uv, do_theta);
 }
 
 // End of a dense step at the absorbing boundary, after the force tiles and
@@ -736,7 +746,7 @@ int enqueue_dense_step(const DenseGeo &dg, const LaunchGeo &lg, const StepPtrs &
       cudaEventRecord(dg.ev_fork[0], st);
       cudaStreamWaitEvent(side, dg.ev_fork[0], 0);
     }
-    k_abc_sell<<<lg.abc.n_slices, 32 * kSellWarps, 0, side>>>(lg.abc, p, 1, gth ? 1 : 0);
+    launch_abc_sell(lg.abc, p, 1, gth ? 1 : 0, side);
     if (mark) (*mark)("abc_sell");
     k++;
     if (fork) cudaEventRecord(dg.ev_join[1], side);
@@ -773,7 +783,7 @@ void launch_abc_theta_dense(const DenseGeo &dg, const LaunchGeo &lg, const doubl
   p.th_np1 = const_cast<double *>(th_n);  // the kernel's "newer" level
   p.th_n = th_nm1;
   p.th_nm1 = th_np1;                       // output slot
-  k_abc_sell<<<lg.abc.n_slices, 32 * kSellWarps, 0, st>>>(lg.abc, p, 0, 1);
+  launch_abc_sell(lg.abc, p, 0, 1, st);
 }
 
 void launch_theta_dense_init(const DenseGeo &, const LaunchGeo &lg, const double2 *u, double *theta,
