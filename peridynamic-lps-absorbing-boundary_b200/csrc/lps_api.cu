@@ -610,11 +610,8 @@ int build_dense(lps_handle *h, const lps_problem *probs, const std::vector<Latti
             const long c = first + (long)r * P + q;
             if (!(type[c] & kExists)) continue;
             any = true;
-            bool cell_full = true;
-            for (size_t j = 0; j < A.size() && cell_full; j++)
-              if (!(type[c + (long)A[j] * P + B[j]] & kExists)) cell_full = false;
-            if (cell_full) type[c] |= kFullHorizon;  // the per-cell kernels skip the neighbour checks
-            full = full && cell_full;
+            for (size_t j = 0; j < A.size() && full; j++)
+              if (!(type[c + (long)A[j] * P + B[j]] & kExists)) full = false;
           }
         if (any)
           tiles.push_back(DenseTile{region_row, region_col, k, full ? kTileFull : 0});

@@ -457,13 +457,12 @@ __global__ void __launch_bounds__(256) k_abc_predict(Abc ab, StepPtrs p) {
 template <int M>
 __device__ __forceinline__ double theta_cell(const Geo &g, const double2 *u, size_t cell, int pitch) {
   const double2 ui = u[cell];
-  const bool full = g.type[cell] & kFullHorizon;  // every neighbour exists
   double s0 = 0.0, s1 = 0.0;
   static_for<0, Sten<M>::N>([&](auto jc) {
     constexpr int j = decltype(jc)::value;
     constexpr int a = make_sten<M>().a[j], b = make_sten<M>().b[j];
     const size_t nb = (size_t)((ptrdiff_t)cell + (ptrdiff_t)a * pitch + b);
-    if (full || (g.type[nb] & kExists)) {
+    if (g.type[nb] & kExists) {
       const double2 uj = u[nb];
       s0 = fma(SC<M>(5, j), uj.x - ui.x, s0);
       s1 = fma(SC<M>(6, j), uj.y - ui.y, s1);
@@ -492,13 +491,12 @@ template <int M>
 __device__ __forceinline__ void wdev_cell(const Geo &g, const double2 *u, size_t cell, int pitch, double th,
                                           double coef, double *W) {
   const double2 ui = u[cell];
-  const bool full = g.type[cell] & kFullHorizon;  // every neighbour exists
   double w = 0.0;
   static_for<0, Sten<M>::N>([&](auto jc) {
     constexpr int j = decltype(jc)::value;
     constexpr int a = make_sten<M>().a[j], b = make_sten<M>().b[j];
     const size_t nb = (size_t)((ptrdiff_t)cell + (ptrdiff_t)a * pitch + b);
-    if (full || (g.type[nb] & kExists)) {
+    if (g.type[nb] & kExists) {
       const double2 uj = u[nb];
       const double e = SC<M>(0, j) * (uj.x - ui.x) + SC<M>(1, j) * (uj.y - ui.y);
       const double ed = e - th * SC<M>(2, j) / 2.0;
