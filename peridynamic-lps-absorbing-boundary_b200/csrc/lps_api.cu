@@ -620,6 +620,16 @@ int build_dense(lps_handle *h, const lps_problem *probs, const std::vector<Latti
   std::stable_sort(tiles.begin(), tiles.end(), [&](const DenseTile &x, const DenseTile &y) {
     return lat[x.inst].M < lat[y.inst].M;
   });
+  // each instance's tiles are contiguous (sorted by m, stable): its range
+  for (int k = 0; k < K; k++) {
+    h->params[k].tile_begin = 0;
+    h->params[k].tile_count = 0;
+  }
+  for (int i = (int)tiles.size() - 1; i >= 0; i--) {
+    InstParams &Pk = h->params[tiles[i].inst];
+    Pk.tile_begin = i;
+    Pk.tile_count++;
+  }
   D.groups.clear();
   for (int i = 0; i < (int)tiles.size(); i++) {
     const int M = lat[tiles[i].inst].M;
@@ -766,14 +776,16 @@ int enqueue_step(lps_handle *h, int64_t n, bool diag, const Mark *mark = nullptr
       M("merge_abc");
       k++;
     }
-    if (h->path == LPS_PATH_DENSE)
-      launch_diag_dense(h->dg, h->lg, p.u_np1, p.v_np1, p.a_np1, p.th_np1, h->partials, h->log,
-                        h->log_count, h->log_capacity, h->d_step, st);
-    else
+    if (h->path == LPS_PATH_DENSE) {
+      launch_diag_dense(h->dg, h->lg, (int)((n + 1) % h->ring_u), p.u_np1, p.v_np1, p.a_np1, p.th_np1,
+                        h->partials, h->log, h->log_count, h->log_capacity, h->d_step, st);
+      k += (int)h->dg.groups.size() + (h->lg.abc.n_abc > 0 ? 1 : 0) + 1;  // tiles per group, ABC, finish
+    } else {
       launch_diag_csr(h->lg, p.u_np1, p.v_np1, p.a_np1, p.th_np1, h->partials, h->log, h->log_count,
                       h->log_capacity, h->d_step, st);
+      k += 2;
+    }
     M("diag");
-    k += 2;
   }
   return k;
 }
@@ -912,7 +924,10 @@ int alloc_state(lps_handle *h) {
       if ((s = dev_alloc(h, &h->U32[r], n))) return s;
       LPS_CUDA_TRY(h, cudaMemset(h->U32[r], 0, sizeof(float2) * n));
     }
-  const int n_part = h->lg.n_node_blocks + (h->n_abc_total + kNodeBlock - 1) / kNodeBlock + 1;
+  // diagnostics partials: node blocks (CSR) or tiles (dense), then ABC blocks
+  int n_tiles = 0;
+  for (const auto &gr : h->dg.groups) n_tiles = std::max(n_tiles, gr.tile_begin + gr.n_tiles);
+  const int n_part = std::max(h->lg.n_node_blocks, n_tiles) + (h->n_abc_total + kNodeBlock - 1) / kNodeBlock + 1;
   h->log_capacity = 1024;
   if ((s = dev_alloc(h, &h->partials, n_part)) ||
       (s = dev_alloc(h, &h->log, (size_t)h->n_inst * h->log_capacity)) ||

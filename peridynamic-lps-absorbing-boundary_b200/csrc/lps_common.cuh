@@ -15,9 +15,10 @@ __device__ __forceinline__ double warp_sum(double v) {
   return __shfl_sync(0xffffffffu, v, 0);
 }
 
-// Accumulator of the diagnostics of src/main.cpp:986-1062.  Combining keeps
-// node order (left = lower node indices), so the argmax ties resolve to the
-// first node, as the strict '>' scan of :1000-1001 does.
+// Accumulator of the diagnostics of src/main.cpp:986-1062.  Equal maxima
+// resolve to the lower node index, so the argmax is the first node whatever
+// the order of combining, as the strict '>' scan of :1000-1001 finds it
+// (node index order is cell index order on both paths).
 struct DiagAcc {
   double E, Ek, Ep, Px, Py, max_u, max_v, max_a, th_min, th_max, uB, vB;
   int iu, iv, nact;
@@ -35,18 +36,18 @@ struct DiagAcc {
     const double um = sqrt(u.x * u.x + u.y * u.y);
     const double vm = sqrt(v.x * v.x + v.y * v.y);
     const double am = sqrt(a.x * a.x + a.y * a.y);
-    if (um > max_u) { max_u = um; iu = idx; }
-    if (vm > max_v) { max_v = vm; iv = idx; }
+    if (um > max_u || (um == max_u && iu >= 0 && idx < iu)) { max_u = um; iu = idx; }
+    if (vm > max_v || (vm == max_v && iv >= 0 && idx < iv)) { max_v = vm; iv = idx; }
     max_a = (max_a < am) ? am : max_a;      // std::max(max_a, a_mag)
     th_min = (th < th_min) ? th : th_min;   // std::min(theta_min, theta)
     th_max = (th_max < th) ? th : th_max;   // std::max(theta_max, theta)
   }
-  // this = this (+) r, where r covers later nodes
+  // this = this (+) r
   __device__ __forceinline__ void combine(const DiagAcc &r) {
     E += r.E; Ek += r.Ek; Ep += r.Ep; Px += r.Px; Py += r.Py;
     uB += r.uB; vB += r.vB; nact += r.nact;
-    if (r.max_u > max_u) { max_u = r.max_u; iu = r.iu; }
-    if (r.max_v > max_v) { max_v = r.max_v; iv = r.iv; }
+    if (r.max_u > max_u || (r.max_u == max_u && r.iu >= 0 && (iu < 0 || r.iu < iu))) { max_u = r.max_u; iu = r.iu; }
+    if (r.max_v > max_v || (r.max_v == max_v && r.iv >= 0 && (iv < 0 || r.iv < iv))) { max_v = r.max_v; iv = r.iv; }
     max_a = (max_a < r.max_a) ? r.max_a : max_a;
     th_min = (r.th_min < th_min) ? r.th_min : th_min;
     th_max = (th_max < r.th_max) ? r.th_max : th_max;
@@ -107,5 +108,10 @@ struct DiagAcc {
 // its ABC blocks (in order) into one record appended to the instance's log.
 void launch_diag_finish(int n_inst, const DiagPartial *partials, int n_node_blocks, DiagRecord *log,
                         int *log_count, int log_capacity, const int *d_step, cudaStream_t st);
+// The same for the dense path's tile partials: instance k folds its tiles
+// [tile_begin, tile_begin + tile_count) and then its ABC blocks, which follow
+// the n_tiles tile partials.
+void launch_diag_finish_tiles(int n_inst, const DiagPartial *partials, int n_tiles, DiagRecord *log,
+                              int *log_count, int log_capacity, const int *d_step, cudaStream_t st);
 
 }  // namespace lps

@@ -119,7 +119,8 @@ void launch_abc_theta_dense(const DenseGeo &dg, const LaunchGeo &lg, const doubl
                             double *th_np1, cudaStream_t st);
 void launch_theta_dense_init(const DenseGeo &dg, const LaunchGeo &lg, const double2 *u, double *theta,
                              cudaStream_t st);
-void launch_diag_dense(const DenseGeo &dg, const LaunchGeo &lg, const double2 *u, const double2 *v,
+// Diagnostics of the level u = ring_u (its TMA descriptor) with v, a, theta.
+void launch_diag_dense(const DenseGeo &dg, const LaunchGeo &lg, int ring_u, const double2 *u, const double2 *v,
                        const double2 *a, const double *theta, DiagPartial *partials, DiagRecord *log,
                        int *log_count, int log_capacity, const int *d_step, cudaStream_t st);
 

@@ -22,7 +22,7 @@
 
 namespace lps {
 
-constexpr int kMaxInstances = 128;   // entries of the __constant__ table (192 B each)
+constexpr int kMaxInstances = 128;   // entries of the __constant__ table (200 B each)
 constexpr int kNodeBlock = 256;      // threads per node-kernel block
 constexpr int kAbcWarpsPerBlock = 8; // warps per ABC block (one ABC node each)
 
@@ -53,7 +53,7 @@ struct InstParams {
   int dense;                    // 1 = dense grid layout
   int pitch, nrow, ncol;        // dense grid geometry (pitch in cells)
   int stencil;                  // dense: stencil-class id
-  int pad0;
+  int tile_begin, tile_count;   // dense: the instance's tiles in the tile list
 };
 
 // Buffer pointers of one time step, resolved on the host from the ring phase.

@@ -486,65 +486,112 @@ __global__ void __launch_bounds__(256) k_theta_dense_init(Geo g, const double2 *
   theta[cell] = th;
 }
 
-// Deviatoric strain-energy sum of one cell, src/main.cpp:1025-1038.
+// Diagnostics of the dense path (src/main.cpp:986-1062), one CTA per tile:
+// the tile's displacements and node types are staged with TMA (as for the
+// dilatation), and each thread sums the deviatoric strain energy of its two
+// cells over the opposite-offset pairs -- for offset (a, b) the bond
+// extension e+ = xi_hat . (u(+) - u_i), for (-a, -b) it is
+// e- = xi_hat . (u_i - u(-)), each with e^d = e - theta_i |xi| / 2 (:1027-1038)
+// -- then kinetic energy, momentum and the maxima from its own cells.  Each
+// tile leaves one partial; k_diag_abc adds the boundary norms (:1050-1062).
 template <int M>
-__device__ __forceinline__ void wdev_cell(const Geo &g, const double2 *u, size_t cell, int pitch, double th,
-                                          double coef, double *W) {
-  const double2 ui = u[cell];
-  double w = 0.0;
-  static_for<0, Sten<M>::N>([&](auto jc) {
-    constexpr int j = decltype(jc)::value;
-    constexpr int a = make_sten<M>().a[j], b = make_sten<M>().b[j];
-    const size_t nb = (size_t)((ptrdiff_t)cell + (ptrdiff_t)a * pitch + b);
-    if (g.type[nb] & kExists) {
-      const double2 uj = u[nb];
-      const double e = SC<M>(0, j) * (uj.x - ui.x) + SC<M>(1, j) * (uj.y - ui.y);
-      const double ed = e - th * SC<M>(2, j) / 2.0;
-      const double bdv = SC<M>(3, j) * SC<M>(0, j) + SC<M>(4, j) * SC<M>(1, j);
-      w += coef * ed * ed * bdv;
-    }
-  });
-  *W = w;
-}
-
-__global__ void __launch_bounds__(kNodeBlock)
-    k_diag_dense(Geo g, Abc ab, const double2 *__restrict__ u, const double2 *__restrict__ v,
-                 const double2 *__restrict__ a, const double *__restrict__ theta, DiagPartial *partials,
-                 int n_node_blocks) {
+__global__ void __launch_bounds__(kTileThreads, 2)
+    k_diag_tiles(const __grid_constant__ CUtensorMap map_u, const __grid_constant__ CUtensorMap map_type, Geo g,
+                 const DenseTile *__restrict__ tiles, int tile_begin, const double2 *__restrict__ v,
+                 const double2 *__restrict__ acc_n, const double *__restrict__ theta, DiagPartial *partials,
+                 int pitch, int *err) {
+  using R = Region<M>;
+  static_assert(R::THETA_STAGE + 64 <= 48 * 1024, "one stage fits the default shared-memory limit");
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem + R::THETA_STAGE);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const DenseTile t = tiles[tile_begin + blockIdx.x];
   DiagAcc acc;
   acc.init();
-  if ((int)blockIdx.x >= n_node_blocks) {
-    const int e = (blockIdx.x - n_node_blocks) * kNodeBlock + threadIdx.x;
-    if (e < ab.n_abc && ab.active[e]) {
-      const int node = ab.node[e];
-      const double2 un = u[node], vn = v[node];
-      acc.uB = un.x * un.x + un.y * un.y;
-      acc.vB = vn.x * vn.x + vn.y * vn.y;
-      acc.nact = 1;
-    }
-    acc.block_reduce_store(partials + blockIdx.x);
-    return;
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    mbar_fence_init();
+    mbar_expect_tx(bar, R::THETA_TX);
+    tma_load_2d(smem, &map_u, 2 * t.col, t.row, bar);
+    tma_load_2d(smem + R::T_TY, &map_type, t.col, t.row, bar);
   }
-  const size_t cell = (size_t)blockIdx.x * kNodeBlock + threadIdx.x;
-  if (cell < (size_t)g.n_total && (g.type[cell] & kExists)) {
-    const InstParams &P = c_inst[g.blk_inst[blockIdx.x]];
-    const double2 xy = g.xy[cell], un = u[cell], vn = v[cell], an = a[cell];
-    const double th = theta[cell];
-    const double r = sqrt(xy.x * xy.x + xy.y * xy.y);
-    acc.add_maxima(un, vn, an, th, (int)cell);
-    if (!(P.out_r > 0.0 && r > P.out_r)) {
-      acc.Px = P.rho * vn.x * P.dx * P.dy;
-      acc.Py = P.rho * vn.y * P.dx * P.dy;
-      const double ek = 0.5 * P.rho * (vn.x * vn.x + vn.y * vn.y) * P.dx * P.dy;
-      const double coef = P.c_mu4 / g.m[cell];
-      double W = 0.0;
-      LPS_DISPATCH_M(P.stencil, wdev_cell, g, u, cell, P.pitch, th, coef, &W);
-      const double W_i = 0.5 * P.kappa * th * th + W;
+  const InstParams &P = c_inst[t.inst];
+  const int r0 = 2 * warp;
+  const size_t cell0 = (size_t)(t.row + M + r0) * pitch + t.col + M + lane;
+  // the owned cells' other fields, fetched while the copy lands
+  double2 vv[2], aa[2], xy[2];
+  double th[2], mi[2];
+#pragma unroll
+  for (int k = 0; k < 2; k++) {
+    const size_t cell = cell0 + (size_t)k * pitch;
+    vv[k] = v[cell];
+    aa[k] = acc_n[cell];
+    xy[k] = g.xy[cell];
+    th[k] = theta[cell];
+    mi[k] = g.m[cell];
+  }
+  __syncthreads();  // barrier initialised before any thread waits on it
+  const bool ok = mbar_wait_bounded(bar, 0, err);
+  const double2 *su = reinterpret_cast<const double2 *>(smem);
+  const uint8_t *sty = smem + R::T_TY;
+  if (ok) {
+    const bool full = t.flags & kTileFull;
+    const double2 ui[2] = {su[QI<M>(r0, lane)], su[QI<M>(r0 + 1, lane)]};
+    double w[2] = {0.0, 0.0};
+    for_each_pair<M>(
+        [&](auto ac, auto bc) {
+          constexpr int a = decltype(ac)::value, b = decltype(bc)::value;
+          constexpr int j = sten_index(M, a, b);
+          const double hx = SC<M>(0, j), hy = SC<M>(1, j), L = SC<M>(2, j);
+          const double bdv = SC<M>(3, j) * SC<M>(0, j) + SC<M>(4, j) * SC<M>(1, j);  // beta dV
+#pragma unroll
+          for (int k = 0; k < 2; k++) {
+            const int r = r0 + k;
+            const double2 up = su[QI<M>(r + a, lane + b)], um = su[QI<M>(r - a, lane - b)];
+            const double hl = th[k] * L / 2.0;
+            const double e1 = hx * (up.x - ui[k].x) + hy * (up.y - ui[k].y) - hl;
+            const double e2 = hx * (ui[k].x - um.x) + hy * (ui[k].y - um.y) - hl;
+            if (full) {
+              w[k] += bdv * (e1 * e1 + e2 * e2);
+            } else {
+              if (sty[(r + a + M) * R::RT + lane + b + M] & kExists) w[k] += bdv * (e1 * e1);
+              if (sty[(r - a + M) * R::RT + lane - b + M] & kExists) w[k] += bdv * (e2 * e2);
+            }
+          }
+        },
+        [](auto) {});
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+      if (!(sty[(r0 + k + M) * R::RT + lane + M] & kExists)) continue;
+      const size_t cell = cell0 + (size_t)k * pitch;
+      acc.add_maxima(ui[k], vv[k], aa[k], th[k], (int)cell);
+      const double rr = sqrt(xy[k].x * xy[k].x + xy[k].y * xy[k].y);
+      if (P.out_r > 0.0 && rr > P.out_r) continue;  // energy only in the near field (:1010)
+      acc.Px += P.rho * vv[k].x * P.dx * P.dy;
+      acc.Py += P.rho * vv[k].y * P.dx * P.dy;
+      const double ek = 0.5 * P.rho * (vv[k].x * vv[k].x + vv[k].y * vv[k].y) * P.dx * P.dy;
+      const double W_i = 0.5 * P.kappa * th[k] * th[k] + (P.c_mu4 / mi[k]) * w[k];
       const double ep = W_i * P.dx * P.dy;
-      acc.Ek = ek;
-      acc.Ep = ep;
-      acc.E = ek + ep;
+      acc.Ek += ek;
+      acc.Ep += ep;
+      acc.E += ek + ep;
     }
+  }
+  acc.block_reduce_store(partials + tile_begin + blockIdx.x);
+}
+
+// Boundary norms at the active ABC nodes (src/main.cpp:1050-1062).
+__global__ void __launch_bounds__(kNodeBlock)
+    k_diag_abc(Abc ab, const double2 *__restrict__ u, const double2 *__restrict__ v, DiagPartial *partials) {
+  DiagAcc acc;
+  acc.init();
+  const int e = blockIdx.x * kNodeBlock + threadIdx.x;
+  if (e < ab.n_abc && ab.active[e]) {
+    const int node = ab.node[e];
+    const double2 un = u[node], vn = v[node];
+    acc.uB = un.x * un.x + un.y * un.y;
+    acc.vB = vn.x * vn.x + vn.y * vn.y;
+    acc.nact = 1;
   }
   acc.block_reduce_store(partials + blockIdx.x);
 }
@@ -791,13 +838,24 @@ void launch_theta_dense_init(const DenseGeo &, const LaunchGeo &lg, const double
   k_theta_dense_init<<<lg.n_node_blocks, 256, 0, st>>>(lg.geo, u, theta);
 }
 
-void launch_diag_dense(const DenseGeo &, const LaunchGeo &lg, const double2 *u, const double2 *v,
+template <int M>
+static void diag_group(const DenseGroup &gr, const LaunchGeo &lg, const DenseGeo &dg, int ring_u, const double2 *v,
+                       const double2 *a, const double *theta, DiagPartial *partials, cudaStream_t st) {
+  k_diag_tiles<M><<<gr.n_tiles, kTileThreads, Region<M>::THETA_STAGE + 64, st>>>(
+      gr.maps.u[ring_u], gr.maps.type, lg.geo, dg.tiles, gr.tile_begin, v, a, theta, partials, dg.pitch, dg.d_err);
+}
+
+void launch_diag_dense(const DenseGeo &dg, const LaunchGeo &lg, int ring_u, const double2 *u, const double2 *v,
                        const double2 *a, const double *theta, DiagPartial *partials, DiagRecord *log,
                        int *log_count, int log_capacity, const int *d_step, cudaStream_t st) {
+  int n_tiles = 0;
+  for (const auto &gr : dg.groups) {
+    LPS_DISPATCH_M(gr.m, diag_group, gr, lg, dg, ring_u, v, a, theta, partials, st);
+    n_tiles = std::max(n_tiles, gr.tile_begin + gr.n_tiles);
+  }
   const int abc_blocks = (lg.abc.n_abc + kNodeBlock - 1) / kNodeBlock;
-  k_diag_dense<<<lg.n_node_blocks + abc_blocks, kNodeBlock, 0, st>>>(lg.geo, lg.abc, u, v, a, theta, partials,
-                                                                      lg.n_node_blocks);
-  launch_diag_finish(lg.n_inst, partials, lg.n_node_blocks, log, log_count, log_capacity, d_step, st);
+  if (abc_blocks > 0) k_diag_abc<<<abc_blocks, kNodeBlock, 0, st>>>(lg.abc, u, v, partials + n_tiles);
+  launch_diag_finish_tiles(lg.n_inst, partials, n_tiles, log, log_count, log_capacity, d_step, st);
 }
 
 }  // namespace lps
