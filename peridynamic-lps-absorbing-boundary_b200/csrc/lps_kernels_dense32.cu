@@ -56,6 +56,30 @@ __host__ __device__ constexpr float sten_q(int Q, int M, int a, int b) {
 template <int M>
 using Region32 = Region<M, 8, 8>;
 
+// Two FP32 values in one 64-bit register pair, for Blackwell's paired FP32
+// instructions (add/sub/fma .f32x2: one instruction for the x and y parts).
+typedef unsigned long long f32x2;
+__device__ __forceinline__ f32x2 f2_pack(float lo, float hi) {
+  f32x2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ float2 f2_unpack(f32x2 v) {
+  float2 r;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(v));
+  return r;
+}
+__device__ __forceinline__ f32x2 f2_sub(f32x2 a, f32x2 b) {
+  f32x2 r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f32x2 f2_fma(f32x2 a, f32x2 b, f32x2 c) {
+  f32x2 r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+
 // s + x with Kahan's running compensation c (the estimate is s - c).
 __device__ __forceinline__ void kahan_add(float &s, float &c, float x) {
   const float y = x - c;
@@ -64,39 +88,40 @@ __device__ __forceinline__ void kahan_add(float &s, float &c, float x) {
   s = t;
 }
 
-// Thread owns cells (r0, c) and (r0 + 1, c), as in the FP64 form.
+// Thread owns cells (r0, c) and (r0 + 1, c), as in the FP64 form.  The x and
+// y parts of a bond pair's displacement difference and of the column's
+// partial sums travel together in paired FP32 instructions.
 template <int M, bool FULL>
 __device__ __forceinline__ void theta_tile32(const float2 *__restrict__ su, const uint8_t *__restrict__ sty, int r0,
                                              int c, float th[2]) {
   using R = Region32<M>;
-  const float2 ui0 = su[QI<M>(r0, c)], ui1 = su[QI<M>(r0 + 1, c)];
-  float S[2] = {0.f, 0.f}, C[2] = {0.f, 0.f}, part[2] = {0.f, 0.f};
+  const f32x2 *__restrict__ sp = reinterpret_cast<const f32x2 *>(su);
+  const f32x2 ui[2] = {sp[QI<M>(r0, c)], sp[QI<M>(r0 + 1, c)]};
+  float S[2] = {0.f, 0.f}, C[2] = {0.f, 0.f};
+  f32x2 part[2] = {0ull, 0ull};  // (x, y) partial sums of the column
   for_each_pair<M>(
       [&](auto ac, auto bc) {
         constexpr int a = decltype(ac)::value, b = decltype(bc)::value;
-        constexpr float wx = sten_q(kWx, M, a, b), wy = sten_q(kWy, M, a, b);
+        const f32x2 w = f2_pack(sten_q(kWx, M, a, b), sten_q(kWy, M, a, b));
 #pragma unroll
         for (int k = 0; k < 2; k++) {
           const int r = r0 + k;
-          const float2 up = su[QI<M>(r + a, c + b)], um = su[QI<M>(r - a, c - b)];
-          float dx = up.x - um.x, dy = up.y - um.y;
+          f32x2 d = f2_sub(sp[QI<M>(r + a, c + b)], sp[QI<M>(r - a, c - b)]);
           if (!FULL) {
             // absent neighbours hold u = 0; restore the -u_i of the present side
             const float mp = (sty[(r + a + M) * R::RT + c + b + M] & kExists) ? 1.f : 0.f;
             const float mm = (sty[(r - a + M) * R::RT + c - b + M] & kExists) ? 1.f : 0.f;
-            const float2 ui = k == 0 ? ui0 : ui1;
-            dx = fmaf(mm - mp, ui.x, dx);
-            dy = fmaf(mm - mp, ui.y, dy);
+            d = f2_fma(f2_pack(mm - mp, mm - mp), ui[k], d);
           }
-          part[k] = fmaf(wx, dx, part[k]);
-          part[k] = fmaf(wy, dy, part[k]);
+          part[k] = f2_fma(w, d, part[k]);
         }
       },
       [&](auto) {
 #pragma unroll
         for (int k = 0; k < 2; k++) {
-          kahan_add(S[k], C[k], part[k]);
-          part[k] = 0.f;
+          const float2 pk = f2_unpack(part[k]);
+          kahan_add(S[k], C[k], pk.x + pk.y);
+          part[k] = 0ull;
         }
       });
   th[0] = S[0] - C[0];
@@ -106,12 +131,14 @@ __device__ __forceinline__ void theta_tile32(const float2 *__restrict__ su, cons
 template <int M, bool FULL>
 __device__ __forceinline__ void force_tile32(const float2 *__restrict__ su, const float2 *__restrict__ sab, int r0,
                                              int c, float F[2][2]) {
-  float2 ui[2], ab_i[2];
+  const f32x2 *__restrict__ sp = reinterpret_cast<const f32x2 *>(su);
+  f32x2 ui[2];
+  float2 ab_i[2];
   float S0[2] = {0.f, 0.f}, C0[2] = {0.f, 0.f}, S1[2] = {0.f, 0.f}, C1[2] = {0.f, 0.f};
   float p0[2] = {0.f, 0.f}, p1[2] = {0.f, 0.f};
 #pragma unroll
   for (int k = 0; k < 2; k++) {
-    ui[k] = su[QI<M>(r0 + k, c)];
+    ui[k] = sp[QI<M>(r0 + k, c)];
     ab_i[k] = sab[QI<M>(r0 + k, c)];
   }
   for_each_pair<M>(
@@ -123,9 +150,11 @@ __device__ __forceinline__ void force_tile32(const float2 *__restrict__ su, cons
         for (int k = 0; k < 2; k++) {
           const int r = r0 + k;
           const int qp = QI<M>(r + a, c + b), qm = QI<M>(r - a, c - b);
-          const float2 up = su[qp], um = su[qm], abp = sab[qp], abm = sab[qm];
-          const float e1 = fmaf(hx, up.x - ui[k].x, hy * (up.y - ui[k].y));
-          const float e2 = fmaf(hx, ui[k].x - um.x, hy * (ui[k].y - um.y));
+          const float2 abp = sab[qp], abm = sab[qm];
+          const float2 d1 = f2_unpack(f2_sub(sp[qp], ui[k]));  // u(+) - u_i
+          const float2 d2 = f2_unpack(f2_sub(ui[k], sp[qm]));  // u_i - u(-)
+          const float e1 = fmaf(hx, d1.x, hy * d1.y);
+          const float e2 = fmaf(hx, d2.x, hy * d2.y);
           float T, wp, wm;
           if (FULL) {
             T = (abp.x - abm.x) * L;
