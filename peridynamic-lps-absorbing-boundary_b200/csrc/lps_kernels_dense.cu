@@ -189,7 +189,7 @@ __device__ __forceinline__ void force_tile(const double2 *__restrict__ su, const
 // ---------------------------------------------------------------------------
 // Predicted displacements -> dilatation, persistent over tiles.
 template <int M>
-__global__ void __launch_bounds__(kTileThreads, 2)
+__global__ void __launch_bounds__(kTileThreads, 3)
     k_theta_tma(const __grid_constant__ CUtensorMap map_u, const __grid_constant__ CUtensorMap map_type, Geo g,
                 const DenseTile *__restrict__ tiles, int tile_begin, int n_tiles, StepPtrs p, int pitch,
                 int skip_abc, int *sched, int *err) {
@@ -642,9 +642,7 @@ static cudaError_t prepare_m(DenseGroup &gr, int n_sm) {
     return e;
   bt = std::max(bt, 1);
   bf = std::max(bf, 1);
-  // at most 2 theta CTAs per SM: the rest of the SM runs the concurrent
-  // absorbing-boundary kernel of the same step
-  gr.grid_theta = std::min(gr.n_tiles, std::min(bt, 2) * n_sm);
+  gr.grid_theta = std::min(gr.n_tiles, bt * n_sm);
   gr.grid_force = std::min(gr.n_tiles, bf * n_sm);
   return cudaSuccess;
 }

@@ -191,7 +191,7 @@ __device__ __forceinline__ void force_tile32(const float2 *__restrict__ su, cons
 // ---------------------------------------------------------------------------
 // Predicted displacements (FP32 copy) -> dilatation, persistent over tiles.
 template <int M>
-__global__ void __launch_bounds__(kTileThreads, 2)
+__global__ void __launch_bounds__(kTileThreads, 4)
     k_theta32(const __grid_constant__ CUtensorMap map_u, const __grid_constant__ CUtensorMap map_type, Geo g,
               const DenseTile *__restrict__ tiles, int tile_begin, int n_tiles, StepPtrs p, int pitch, int skip_abc,
               int *sched, int *err) {
