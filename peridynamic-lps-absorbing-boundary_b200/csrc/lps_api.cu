@@ -58,7 +58,6 @@ struct lps_handle {
 
   // state
   double2 *U[kUring] = {}, *V[3] = {}, *A[2] = {}, *VH = nullptr, *S = nullptr;
-  double2 *S1 = nullptr;      // dense path: second G_u result buffer (step parity)
   int ring_u = 3;             // displacement ring depth: 3 (CSR path) or 4 (dense path)
   double *TH[3] = {};
   double2 *U0 = nullptr, *V0 = nullptr;
@@ -730,15 +729,7 @@ StepPtrs step_ptrs(lps_handle *h, int64_t n) {
   p.th_np1 = h->TH[u1];
   p.u32_np1 = h->U32[(n + 1) % 2];
   p.u32_np2 = h->U32[n % 2];
-  if (h->path == LPS_PATH_DENSE) {
-    // the dense step computes G_u concurrently with the predictor that still
-    // reads the previous result, so the two alternate by step parity
-    p.s_abc = (n + 1) % 2 ? h->S1 : h->S;
-    p.s_prev = n % 2 ? h->S1 : h->S;
-  } else {
-    p.s_abc = h->S;
-    p.s_prev = h->S;
-  }
+  p.s_abc = h->S;
   return p;
 }
 
@@ -915,7 +906,6 @@ int alloc_state(lps_handle *h) {
     LPS_CUDA_TRY(h, cudaMemset(h->A[r], 0, sizeof(double2) * n));
   }
   if ((s = dev_alloc(h, &h->VH, n)) || (s = dev_alloc(h, &h->S, std::max(h->n_abc_total, 1))) ||
-      (s = dev_alloc(h, &h->S1, std::max(h->n_abc_total, 1))) ||
       (s = dev_alloc(h, &h->U0, n)) || (s = dev_alloc(h, &h->V0, n)))
     return s;
   LPS_CUDA_TRY(h, cudaMemset(h->VH, 0, sizeof(double2) * n));
@@ -1228,7 +1218,7 @@ int lps_download(lps_handle *h, int instance, double *u, double *v, double *a, d
   // the newest level: after step n the current level is n
   const int cur = (int)(n % h->ring_u), cur3 = (int)(n % 3), cura = (int)(n % 2);
   if (h->opt.abcs_step != -1 && h->lg.abc.n_abc > 0)
-    launch_merge_abc(h->lg, h->U[cur], (h->path == LPS_PATH_DENSE && n % 2) ? h->S1 : h->S, h->stream);
+    launch_merge_abc(h->lg, h->U[cur], h->S, h->stream);
   LPS_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   if (int e = check_device_error(h)) return e;
   const int nn = h->node_count[instance];

@@ -14,9 +14,11 @@
 //    index (empty cells carry type 0).  See lps_dense.cuh.
 //
 // State is FP64 double2 per node (x, y), in rings so that no step copies
-// data: u and v keep three time levels (n-1, n, n+1: the ABC operators read
-// two history levels, src/main.cpp:903-912), a two, theta three (the G_theta
-// history, :1157-1163).
+// data: v keeps three time levels (n-1, n, n+1: the ABC operators read two
+// history levels, src/main.cpp:903-912), u three (CSR) or four (dense: the
+// force pass already writes the next step's predicted level), a two, theta
+// three (the G_theta history, :1157-1163).  The FP32-mixed form adds an FP32
+// copy of the predicted displacement (two levels).
 #pragma once
 #include <cstdint>
 
@@ -30,7 +32,6 @@ constexpr int kAbcWarpsPerBlock = 8; // warps per ABC block (one ABC node each)
 constexpr uint8_t kExists = 1;       // a real node (not padding)
 constexpr uint8_t kBcAbc = 2;        // BCTypes[2i] == 1 (IDW skips these, :778)
 constexpr uint8_t kActiveAbc = 4;    // overwritten by the G operators this step
-constexpr uint8_t kFullHorizon = 8;  // dense path: every stencil neighbour exists
 
 // Per-instance constants, in __constant__ memory, indexed by instance id.
 struct InstParams {
@@ -58,7 +59,7 @@ struct InstParams {
 
 // Buffer pointers of one time step, resolved on the host from the ring phase.
 struct StepPtrs {
-  double2 *u_n;            // u^n (ABC entries merged in by the predictor)
+  double2 *u_n;            // u^n
   const double2 *u_nm1;    // u^{n-1}
   double2 *u_np1;          // predicted u^{n+1} (ABC nodes: see s_abc)
   const double2 *v_n, *v_nm1;
@@ -68,9 +69,9 @@ struct StepPtrs {
   double2 *vh;             // v^n + dt/2 a^n (first half of the corrector)
   const double *th_n, *th_nm1;
   double *th_np1;
-  double2 *s_abc;          // G_u result u^{n+1} at ABC nodes, merged next step
+  double2 *s_abc;          // G_u result u^{n+1} at ABC nodes (merged into the ring
+                           // by the dense step's end, by the CSR predictor)
   double2 *u_np2;          // dense path: predicted u^{n+2}, written by the force pass
-  const double2 *s_prev;   // dense path: G_u result of the previous step (u^n at ABC nodes)
   float2 *u32_np1;         // FP32-mixed form: FP32 copy of the predicted u^{n+1}
   float2 *u32_np2;         // FP32-mixed form: FP32 copy of u^{n+2}, written by the force pass
   int th_ring;             // ring index of th_np1
