@@ -244,7 +244,7 @@ def run_ours(args, rank, world, local_rank, precision, with_cpu=True):
     sets = workload_sets(args.workload, args.time_steps)
     stream = torch.cuda.Stream(device=dev)
     sv = Solver(sets, precision=precision, path=args.path, device=local_rank,
-                stream=stream.cuda_stream)
+                stream=stream.cuda_stream, autotune=True)
     info = sv.info(0)
     T, K, W = args.time_steps, args.steps, args.warmup
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
@@ -347,7 +347,8 @@ def run_ours(args, rank, world, local_rank, precision, with_cpu=True):
            "e2e": {"value": e2e_value, "unit": "node-steps/s", "h2d_bytes_per_step": h2d,
                    "d2h_bytes_per_step": d2h},
            "gpu_launches": launches, "roofline": roofline, "clocks": clk,
-           "kernel_path": info["path"], "final_dE_rel": final_dE, "_u": final_u}
+           "kernel_path": info["path"], "tile_ctas": [info["tile_ctas_theta"], info["tile_ctas_force"]],
+           "final_dE_rel": final_dE, "_u": final_u}
     if with_cpu and rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         s_cpu = [s for s in sets if abs(s.nu - 0.25) < 1e-12][0] if len(sets) > 1 else sets[0]

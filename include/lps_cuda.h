@@ -89,6 +89,11 @@ typedef struct lps_options {
   int32_t device;           /* CUDA device ordinal                            */
   int32_t use_graphs;       /* 1 (default): replay captured CUDA graphs       */
   void *stream;             /* cudaStream_t to run on, or NULL for an owned one */
+  int32_t autotune;         /* 1: lps_create times the dense tile kernels at  */
+                            /* each resident-CTA count and keeps the fastest  */
+                            /* (no effect on results); 0 (default): maximum   */
+                            /* occupancy                                      */
+  int32_t pad_;
 } lps_options;
 
 /* One output record: the .energy columns (src/main.cpp:1108-1112), the
@@ -108,6 +113,8 @@ typedef struct lps_info {
   int64_t device_bytes;                                       /* allocated    */
   int64_t step;                                               /* steps taken  */
   int32_t n_abc_m_corrected, pad;                             /* instance 0   */
+  int32_t tile_ctas_theta, tile_ctas_force;  /* dense path: CTAs per SM of the */
+                                             /* dilatation / force tiles      */
 } lps_info;
 
 typedef struct lps_handle lps_handle;

@@ -781,6 +781,56 @@ int enqueue_step(lps_handle *h, int64_t n, bool diag, const Mark *mark = nullptr
   return k;
 }
 
+int do_reset(lps_handle *h);
+int check_device_error(lps_handle *h);
+
+// The autotuner of the dense path: times a few eager steps from the initial
+// state at every count of resident dilatation / force CTAs per SM (1 up to
+// the occupancy limit) and keeps the fastest pair.  Grid sizes do not change
+// any result: tiles come from a counter and each cell's arithmetic is the
+// same whichever CTA computes it.  The caller resets the state afterwards.
+int autotune_dense(lps_handle *h) {
+  int max_t = 1, max_f = 1;
+  for (const auto &gr : h->dg.groups) {
+    max_t = std::max(max_t, gr.max_theta_ctas);
+    max_f = std::max(max_f, gr.max_force_ctas);
+  }
+  cudaEvent_t e0, e1;
+  LPS_CUDA_TRY(h, cudaEventCreate(&e0));
+  LPS_CUDA_TRY(h, cudaEventCreate(&e1));
+  const int warm = 2, timed = 8;
+  float best = 1e30f;
+  int best_t = max_t, best_f = max_f;
+  int st = LPS_OK;
+  for (int t = 1; t <= max_t && st == LPS_OK; t++)
+    for (int f = 1; f <= max_f && st == LPS_OK; f++) {
+      dense_set_ctas(h->dg, t, f);
+      if ((st = do_reset(h))) break;
+      for (int n = 0; n < warm; n++) enqueue_step(h, n, false);
+      cudaEventRecord(e0, h->stream);
+      for (int n = warm; n < warm + timed; n++) enqueue_step(h, n, false);
+      cudaEventRecord(e1, h->stream);
+      if (cudaEventSynchronize(e1) != cudaSuccess) {
+        h->err = "autotune: a timing step failed";
+        st = LPS_ERR_CUDA;
+        break;
+      }
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (ms < best) {
+        best = ms;
+        best_t = t;
+        best_f = f;
+      }
+    }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st == LPS_OK) st = check_device_error(h);
+  if (st) return st;
+  dense_set_ctas(h->dg, best_t, best_f);
+  return LPS_OK;
+}
+
 int drain_log(lps_handle *h) {
   if (h->pending_records == 0) return LPS_OK;
   LPS_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
@@ -1102,6 +1152,8 @@ int lps_create(const lps_problem *problems, int n_instances, const lps_options *
     }
   }
   if ((s = do_reset(h))) return fail(s);
+  if (o.autotune && h->path == LPS_PATH_DENSE && (s = autotune_dense(h))) return fail(s);
+  if (o.autotune && h->path == LPS_PATH_DENSE && (s = do_reset(h))) return fail(s);
   if (cudaStreamSynchronize(h->stream) != cudaSuccess) {
     h->err = std::string("setup kernels failed: ") + cudaGetErrorString(cudaGetLastError());
     return fail(LPS_ERR_CUDA);
@@ -1288,6 +1340,14 @@ int lps_get_info(lps_handle *h, int instance, lps_info *info) {
   info->device_bytes = h->device_bytes;
   info->step = h->step;
   info->n_abc_m_corrected = s.n_corrected;
+  if (h->path == LPS_PATH_DENSE && !h->dg.groups.empty()) {
+    int dev = 0, n_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+    const DenseGroup &g0 = h->dg.groups[0];
+    info->tile_ctas_theta = (g0.grid_theta + n_sm - 1) / n_sm;
+    info->tile_ctas_force = (g0.grid_force + n_sm - 1) / n_sm;
+  }
   return LPS_OK;
 }
 

@@ -59,6 +59,7 @@ struct DenseGroup {
   int n_tiles;
   int grid_theta;   // persistent grid sizes
   int grid_force;
+  int max_theta_ctas, max_force_ctas;  // resident CTAs per SM at full occupancy
   int *sched;       // device tile-scheduler counters (theta: [0..1], force: [2..3])
   DenseMaps maps;
 };
@@ -97,6 +98,9 @@ int dense_encode_maps(DenseGroup &g, int pitch, int total_rows, double2 *const *
                       std::string &err);
 // Sets shared-memory limits and the persistent grid sizes of each group.
 cudaError_t dense_prepare(DenseGeo &dg);
+// Persistent grids of every group at the given resident CTAs per SM (each
+// clamped to 1..the group's occupancy limit).
+void dense_set_ctas(DenseGeo &dg, int theta_ctas, int force_ctas);
 
 // FP32-mixed tile kernels (lps_kernels_dense32.cu): shared-memory limits,
 // persistent grids and launches of one group.

@@ -644,12 +644,26 @@ static cudaError_t prepare_m(DenseGroup &gr, int n_sm) {
   bf = std::max(bf, 1);
   gr.grid_theta = std::min(gr.n_tiles, bt * n_sm);
   gr.grid_force = std::min(gr.n_tiles, bf * n_sm);
+  gr.max_theta_ctas = bt;
+  gr.max_force_ctas = bf;
   return cudaSuccess;
 }
 
 template <int M>
 static void prepare_dispatch(DenseGroup &gr, int n_sm, cudaError_t *e) {
   *e = prepare_m<M>(gr, n_sm);
+}
+
+void dense_set_ctas(DenseGeo &dg, int theta_ctas, int force_ctas) {
+  int dev = 0, n_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+  for (auto &gr : dg.groups) {
+    const int t = std::max(1, std::min(theta_ctas, gr.max_theta_ctas));
+    const int f = std::max(1, std::min(force_ctas, gr.max_force_ctas));
+    gr.grid_theta = std::min(gr.n_tiles, t * n_sm);
+    gr.grid_force = std::min(gr.n_tiles, f * n_sm);
+  }
 }
 
 cudaError_t dense_prepare(DenseGeo &dg) {

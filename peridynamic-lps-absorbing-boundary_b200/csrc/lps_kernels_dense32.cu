@@ -382,6 +382,8 @@ static void prepare32_m(DenseGroup &gr, int n_sm, cudaError_t *out) {
   bf = std::max(bf, 1);
   gr.grid_theta = std::min(gr.n_tiles, bt * n_sm);
   gr.grid_force = std::min(gr.n_tiles, bf * n_sm);
+  gr.max_theta_ctas = bt;
+  gr.max_force_ctas = bf;
 }
 
 cudaError_t dense32_prepare_group(DenseGroup &gr, int n_sm) {

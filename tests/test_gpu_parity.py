@@ -153,3 +153,23 @@ def test_horizon_overflow_is_an_error():
     with pytest.raises(LpsError) as e:
         Solver(s, max_horizon=128)   # m=8: 225 entries with self
     assert e.value.status == -2
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32_mixed"])
+def test_autotune_changes_no_result(precision):
+    """The autotuner only picks resident CTAs per SM for the tile kernels:
+    every result is the same bits as with the default grids."""
+    sets = [gen.disc_problem(R=14.0, m=4, nu=0.3, n_steps=40, sigma=3.0),
+            gen.disc_problem(R=11.0, m=3, nu=0.2, n_steps=40, sigma=2.5)]
+    out = {}
+    for tune in (False, True):
+        with Solver(sets, precision=precision, autotune=tune) as sv:
+            sv.step(40, diag_every=10)
+            out[tune] = [(sv.read_diag(k), sv.download(k)) for k in range(len(sets))]
+            info = sv.info(0)
+        assert info["path"] == "dense"
+        assert 1 <= info["tile_ctas_theta"] <= 8 and 1 <= info["tile_ctas_force"] <= 8
+    for k in range(len(sets)):
+        for key in ("u", "v", "a", "theta"):
+            np.testing.assert_array_equal(out[True][k][1][key], out[False][k][1][key])
+        np.testing.assert_array_equal(out[True][k][0]["E"], out[False][k][0]["E"])
