@@ -89,10 +89,10 @@ typedef struct lps_options {
   int32_t device;           /* CUDA device ordinal                            */
   int32_t use_graphs;       /* 1 (default): replay captured CUDA graphs       */
   void *stream;             /* cudaStream_t to run on, or NULL for an owned one */
-  int32_t autotune;         /* 1: lps_create times the dense tile kernels at  */
-                            /* each resident-CTA count and keeps the fastest  */
-                            /* (no effect on results); 0 (default): maximum   */
-                            /* occupancy                                      */
+  int32_t autotune;         /* 1: lps_create times the dense tile kernels'    */
+                            /* step graph at each resident-CTA count and keeps*/
+                            /* the fastest (no effect on results); 0          */
+                            /* (default): maximum occupancy                   */
   int32_t pad_;
 } lps_options;
 
