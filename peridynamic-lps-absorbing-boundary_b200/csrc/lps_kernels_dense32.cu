@@ -91,20 +91,31 @@ __device__ __forceinline__ void kahan_add(float &s, float &c, float x) {
 // Thread owns cells (r0, c) and (r0 + 1, c), as in the FP64 form.  The x and
 // y parts of a bond pair's displacement difference and of the column's
 // partial sums travel together in paired FP32 instructions.
+// The dilatation thread owns kTh32Rows adjacent rows of one column, so a
+// staged value it loads feeds the pairs of up to kTh32Rows cells.
+constexpr int kTh32Rows = 4;
+constexpr int kTh32Threads = kTileRows * kTileCols / kTh32Rows;
+
 template <int M, bool FULL>
 __device__ __forceinline__ void theta_tile32(const float2 *__restrict__ su, const uint8_t *__restrict__ sty, int r0,
-                                             int c, float th[2]) {
+                                             int c, float th[kTh32Rows]) {
   using R = Region32<M>;
+  constexpr int K = kTh32Rows;
   const f32x2 *__restrict__ sp = reinterpret_cast<const f32x2 *>(su);
-  const f32x2 ui[2] = {sp[QI<M>(r0, c)], sp[QI<M>(r0 + 1, c)]};
-  float S[2] = {0.f, 0.f}, C[2] = {0.f, 0.f};
-  f32x2 part[2] = {0ull, 0ull};  // (x, y) partial sums of the column
+  f32x2 ui[K], part[K];  // own displacement; (x, y) partial sums of the column
+  float S[K], C[K];
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    ui[k] = sp[QI<M>(r0 + k, c)];
+    part[k] = 0ull;
+    S[k] = C[k] = 0.f;
+  }
   for_each_pair<M>(
       [&](auto ac, auto bc) {
         constexpr int a = decltype(ac)::value, b = decltype(bc)::value;
         const f32x2 w = f2_pack(sten_q(kWx, M, a, b), sten_q(kWy, M, a, b));
 #pragma unroll
-        for (int k = 0; k < 2; k++) {
+        for (int k = 0; k < K; k++) {
           const int r = r0 + k;
           f32x2 d = f2_sub(sp[QI<M>(r + a, c + b)], sp[QI<M>(r - a, c - b)]);
           if (!FULL) {
@@ -118,14 +129,14 @@ __device__ __forceinline__ void theta_tile32(const float2 *__restrict__ su, cons
       },
       [&](auto) {
 #pragma unroll
-        for (int k = 0; k < 2; k++) {
+        for (int k = 0; k < K; k++) {
           const float2 pk = f2_unpack(part[k]);
           kahan_add(S[k], C[k], pk.x + pk.y);
           part[k] = 0ull;
         }
       });
-  th[0] = S[0] - C[0];
-  th[1] = S[1] - C[1];
+#pragma unroll
+  for (int k = 0; k < K; k++) th[k] = S[k] - C[k];
 }
 
 template <int M, bool FULL>
@@ -191,7 +202,7 @@ __device__ __forceinline__ void force_tile32(const float2 *__restrict__ su, cons
 // ---------------------------------------------------------------------------
 // Predicted displacements (FP32 copy) -> dilatation, persistent over tiles.
 template <int M>
-__global__ void __launch_bounds__(kTileThreads, 4)
+__global__ void __launch_bounds__(kTh32Threads, 6)
     k_theta32(const __grid_constant__ CUtensorMap map_u, const __grid_constant__ CUtensorMap map_type, Geo g,
               const DenseTile *__restrict__ tiles, int tile_begin, int n_tiles, StepPtrs p, int pitch, int skip_abc,
               int *sched, int *err) {
@@ -228,23 +239,24 @@ __global__ void __launch_bounds__(kTileThreads, 4)
     const InstParams &P = c_inst[t.inst];
     const float2 *su = reinterpret_cast<const float2 *>(smem + stage * R::THETA_STAGE);
     const uint8_t *sty = reinterpret_cast<const uint8_t *>(smem + stage * R::THETA_STAGE + R::T_TY);
-    const int r0 = 2 * warp;
+    const int r0 = kTh32Rows * warp;
     const size_t cell0 = (size_t)(t.row + M + r0) * pitch + t.col + M + lane;
-    const double mi0 = g.m[cell0], mi1 = g.m[cell0 + pitch];
+    double mi[kTh32Rows];
+#pragma unroll
+    for (int k = 0; k < kTh32Rows; k++) mi[k] = g.m[cell0 + (size_t)k * pitch];
     if (!mbar_wait_bounded(&bar[stage], (it >> 1) & 1, err)) return;
-    float th[2];
+    float th[kTh32Rows];
     if (t.flags & kTileFull)
       theta_tile32<M, true>(su, sty, r0, lane, th);
     else
       theta_tile32<M, false>(su, sty, r0, lane, th);
     const double scale = 2.0 * P.dx * P.dy * P.dx;
 #pragma unroll
-    for (int k = 0; k < 2; k++) {
+    for (int k = 0; k < kTh32Rows; k++) {
       const uint8_t ty = sty[(r0 + k + M) * R::RT + lane + M];
       if (!(ty & kExists)) continue;
       if (skip_abc && (ty & kActiveAbc)) continue;  // the G_theta kernel writes it
-      const double mi = k == 0 ? mi0 : mi1;
-      p.th_np1[cell0 + (size_t)k * pitch] = (mi > 0.0) ? (scale / mi) * (double)th[k] : 0.0;
+      p.th_np1[cell0 + (size_t)k * pitch] = (mi[k] > 0.0) ? (scale / mi[k]) * (double)th[k] : 0.0;
     }
     fence_proxy_async_smem();
     __syncthreads();  // the stage is refilled at the start of the next-but-one iteration
@@ -373,7 +385,7 @@ static void prepare32_m(DenseGroup &gr, int n_sm, cudaError_t *out) {
     return;
   }
   int bt = 0, bf = 0;
-  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, k_theta32<M>, kTileThreads, R::THETA_SMEM)) ||
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, k_theta32<M>, kTh32Threads, R::THETA_SMEM)) ||
       (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf, k_force32<M>, kTileThreads, R::FORCE_SMEM))) {
     *out = e;
     return;
@@ -397,7 +409,7 @@ static void theta32_m(const DenseGroup &gr, const LaunchGeo &lg, const DenseGeo 
                       int ring_u, bool skip_abc, cudaStream_t st) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(gr.grid_theta);
-  cfg.blockDim = dim3(kTileThreads);
+  cfg.blockDim = dim3(kTh32Threads);
   cfg.dynamicSmemBytes = Region32<M>::THETA_SMEM;
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
