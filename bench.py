@@ -56,6 +56,9 @@ def parse():
     ap.add_argument("--path", default="auto")
     ap.add_argument("--cpu-sample-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep full occupancy instead of searching the tile kernels' resident CTAs at "
+                         "setup (for launch lists whose first launches should be the time steps)")
     return ap.parse_args()
 
 
@@ -244,7 +247,7 @@ def run_ours(args, rank, world, local_rank, precision, with_cpu=True):
     sets = workload_sets(args.workload, args.time_steps)
     stream = torch.cuda.Stream(device=dev)
     sv = Solver(sets, precision=precision, path=args.path, device=local_rank,
-                stream=stream.cuda_stream, autotune=True)
+                stream=stream.cuda_stream, autotune=not args.no_autotune)
     info = sv.info(0)
     T, K, W = args.time_steps, args.steps, args.warmup
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
