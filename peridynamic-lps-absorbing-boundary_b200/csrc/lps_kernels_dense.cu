@@ -92,29 +92,38 @@ cudaError_t upload_dense_constants(int m, double dx, double dy, double delta, cu
 }
 
 // ---------------------------------------------------------------------------
-// Tile compute.  A thread owns cells (r0, c) and (r0 + 1, c); for every pair
-// of opposite offsets (a, b) / (-a, -b) it reads the two staged neighbours of
-// each cell -- the row-(r0+1) reads of one offset are the row-r0 reads of the
-// next, so about half of them come from registers.
+// Tile compute.  A force thread owns cells (r0, c) and (r0 + 1, c), a
+// dilatation thread kThRows rows of column c; for every pair of opposite
+// offsets (a, b) / (-a, -b) it reads the two staged neighbours of each cell --
+// the row-(r0+1) reads of one offset are the row-r0 reads of the next, so
+// most of them come from registers.
 //   dilatation pair:  c_j . (u(+) - u(-))                    (src/main.cpp:757)
 //   force pair:       g_j [ (A+ - A-) |xi| + (B_i + B+) e+ - (B_i + B-) e- ]
 // with e+ = (u(+) - u_i) . xi_hat, e- = (u_i - u(-)) . xi_hat, A = 2(l-m)/m
 // theta, B = 8 mu / m (:857-869).  Masked tiles (near the domain edge) use the
 // same pairs with absent neighbours zeroed: u = A = B = 0 there, and the
 // owned node's own terms are weighted by which side is present.
+// The dilatation thread owns kThRows adjacent rows of one column (the force
+// thread two), so a staged value it loads feeds the pairs of up to kThRows
+// cells; each cell's sums are the same whatever the rows per thread.
+constexpr int kThRows = 4;
+constexpr int kThThreads = kTileRows * kTileCols / kThRows;
+
 template <int M, bool FULL>
 __device__ __forceinline__ void theta_tile(const double2 *__restrict__ su, const uint8_t *__restrict__ sty, int r0,
-                                           int c, double th[2]) {
+                                           int c, double th[kThRows]) {
   using R = Region<M>;
-  const double2 ui0 = su[QI<M>(r0, c)], ui1 = su[QI<M>(r0 + 1, c)];
-  double s00 = 0.0, s01 = 0.0, s10 = 0.0, s11 = 0.0;
+  constexpr int K = kThRows;
+  double s0[K], s1[K];
+#pragma unroll
+  for (int k = 0; k < K; k++) s0[k] = s1[k] = 0.0;
   for_each_pair<M>(
       [&](auto ac, auto bc) {
         constexpr int a = decltype(ac)::value, b = decltype(bc)::value;
         constexpr int j = sten_index(M, a, b);
         const double cx = SC<M>(5, j), cy = SC<M>(6, j);
 #pragma unroll
-        for (int k = 0; k < 2; k++) {
+        for (int k = 0; k < K; k++) {
           const int r = r0 + k;
           const double2 up = su[QI<M>(r + a, c + b)], um = su[QI<M>(r - a, c - b)];
           double dx = up.x - um.x, dy = up.y - um.y;
@@ -122,22 +131,17 @@ __device__ __forceinline__ void theta_tile(const double2 *__restrict__ su, const
             // absent neighbours hold u = 0; restore the -u_i of the present side
             const double mp = (sty[(r + a + M) * R::RT + c + b + M] & kExists) ? 1.0 : 0.0;
             const double mm = (sty[(r - a + M) * R::RT + c - b + M] & kExists) ? 1.0 : 0.0;
-            const double2 ui = k == 0 ? ui0 : ui1;
+            const double2 ui = su[QI<M>(r, c)];
             dx = fma(mm - mp, ui.x, dx);
             dy = fma(mm - mp, ui.y, dy);
           }
-          if (k == 0) {
-            s00 = fma(cx, dx, s00);
-            s01 = fma(cy, dy, s01);
-          } else {
-            s10 = fma(cx, dx, s10);
-            s11 = fma(cy, dy, s11);
-          }
+          s0[k] = fma(cx, dx, s0[k]);
+          s1[k] = fma(cy, dy, s1[k]);
         }
       },
       [](auto) {});
-  th[0] = s00 + s01;
-  th[1] = s10 + s11;
+#pragma unroll
+  for (int k = 0; k < K; k++) th[k] = s0[k] + s1[k];
 }
 
 template <int M, bool FULL>
@@ -189,7 +193,7 @@ __device__ __forceinline__ void force_tile(const double2 *__restrict__ su, const
 // ---------------------------------------------------------------------------
 // Predicted displacements -> dilatation, persistent over tiles.
 template <int M>
-__global__ void __launch_bounds__(kTileThreads, 3)
+__global__ void __launch_bounds__(kThThreads, 4)
     k_theta_tma(const __grid_constant__ CUtensorMap map_u, const __grid_constant__ CUtensorMap map_type, Geo g,
                 const DenseTile *__restrict__ tiles, int tile_begin, int n_tiles, StepPtrs p, int pitch,
                 int skip_abc, int *sched, int *err) {
@@ -227,23 +231,24 @@ __global__ void __launch_bounds__(kTileThreads, 3)
     const DenseTile t = tiles[tile_begin + tile];
     const double2 *su = reinterpret_cast<const double2 *>(smem + stage * R::THETA_STAGE);
     const uint8_t *sty = reinterpret_cast<const uint8_t *>(smem + stage * R::THETA_STAGE + R::T_TY);
-    const int r0 = 2 * warp;
+    const int r0 = kThRows * warp;
     // m_i of the owned cells, fetched while the copy lands
     const size_t cell0 = (size_t)(t.row + M + r0) * pitch + t.col + M + lane;
-    const double mi0 = g.m[cell0], mi1 = g.m[cell0 + pitch];
+    double mi[kThRows];
+#pragma unroll
+    for (int k = 0; k < kThRows; k++) mi[k] = g.m[cell0 + (size_t)k * pitch];
     if (!mbar_wait_bounded(&bar[stage], (it >> 1) & 1, err)) return;
-    double th[2];
+    double th[kThRows];
     if (t.flags & kTileFull)
       theta_tile<M, true>(su, sty, r0, lane, th);
     else
       theta_tile<M, false>(su, sty, r0, lane, th);
 #pragma unroll
-    for (int k = 0; k < 2; k++) {
+    for (int k = 0; k < kThRows; k++) {
       const uint8_t ty = sty[(r0 + k + M) * R::RT + lane + M];
       if (!(ty & kExists)) continue;
       if (skip_abc && (ty & kActiveAbc)) continue;  // the G_theta kernel writes it
-      const double mi = k == 0 ? mi0 : mi1;
-      p.th_np1[cell0 + (size_t)k * pitch] = (mi > 0.0) ? (2.0 / mi) * th[k] : 0.0;
+      p.th_np1[cell0 + (size_t)k * pitch] = (mi[k] > 0.0) ? (2.0 / mi[k]) * th[k] : 0.0;
     }
     fence_proxy_async_smem();
     __syncthreads();  // the stage is refilled at the start of the next-but-one iteration
@@ -636,7 +641,7 @@ static cudaError_t prepare_m(DenseGroup &gr, int n_sm) {
                                 cudaSharedmemCarveoutMaxShared)))
     return e;
   int bt = 0, bf = 0;
-  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, k_theta_tma<M>, kTileThreads, Region<M>::THETA_SMEM)))
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, k_theta_tma<M>, kThThreads, Region<M>::THETA_SMEM)))
     return e;
   if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf, k_force_tma<M>, kTileThreads, Region<M>::FORCE_SMEM)))
     return e;
@@ -748,7 +753,7 @@ static void launch_theta_group(const DenseGroup &gr, const LaunchGeo &lg, const 
                                int ring_u, bool skip_abc, cudaStream_t st) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(gr.grid_theta);
-  cfg.blockDim = dim3(kTileThreads);
+  cfg.blockDim = dim3(kThThreads);
   cfg.dynamicSmemBytes = Region<M>::THETA_SMEM;
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
