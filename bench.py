@@ -351,6 +351,7 @@ def run_ours(args, rank, world, local_rank, precision, with_cpu=True):
                    "d2h_bytes_per_step": d2h},
            "gpu_launches": launches, "roofline": roofline, "clocks": clk,
            "kernel_path": info["path"], "tile_ctas": [info["tile_ctas_theta"], info["tile_ctas_force"]],
+           "tile_rows_theta": info["tile_rows_theta"],
            "final_dE_rel": final_dE, "_u": final_u}
     if with_cpu and rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1

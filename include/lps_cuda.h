@@ -90,10 +90,12 @@ typedef struct lps_options {
   int32_t use_graphs;       /* 1 (default): replay captured CUDA graphs       */
   void *stream;             /* cudaStream_t to run on, or NULL for an owned one */
   int32_t autotune;         /* 1: lps_create times the dense tile kernels'    */
-                            /* step graph at each resident-CTA count and keeps*/
-                            /* the fastest (no effect on results); 0          */
-                            /* (default): maximum occupancy                   */
-  int32_t pad_;
+                            /* step graph at each rows-per-thread choice and  */
+                            /* resident-CTA count and keeps the fastest (no   */
+                            /* effect on results); 0 (default): 4 rows, full  */
+                            /* occupancy                                      */
+  int32_t theta_rows;       /* dense dilatation rows per thread: 0 (default:  */
+                            /* 4, or the autotuner's choice), 2 or 4 (fixed)  */
 } lps_options;
 
 /* One output record: the .energy columns (src/main.cpp:1108-1112), the
@@ -115,6 +117,8 @@ typedef struct lps_info {
   int32_t n_abc_m_corrected, pad;                             /* instance 0   */
   int32_t tile_ctas_theta, tile_ctas_force;  /* dense path: CTAs per SM of the */
                                              /* dilatation / force tiles      */
+  int32_t tile_rows_theta, pad2;             /* dense path: rows per thread of */
+                                             /* the dilatation tiles          */
 } lps_info;
 
 typedef struct lps_handle lps_handle;

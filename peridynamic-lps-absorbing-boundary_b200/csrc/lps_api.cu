@@ -785,17 +785,20 @@ int do_reset(lps_handle *h);
 int check_device_error(lps_handle *h);
 int get_graph(lps_handle *h, int mask, cudaGraphExec_t *out);
 
-// The autotuner of the dense path: for every count of resident dilatation /
-// force CTAs per SM (1 up to the occupancy limit) it captures the 12-step
-// CUDA graph the run will replay and times two replays of it from the
-// initial state (the faster of two tries); a pair replaces the default
-// (full occupancy) only if it is at least 2 % faster.  Grid sizes do not
-// change any result: tiles come from a counter and each cell's arithmetic is
-// the same whichever CTA computes it.  The caller resets the state afterwards.
-int autotune_dense(lps_handle *h) {
-  int max_t = 1, max_f = 1;
+// The autotuner of the dense path: for each number of rows a dilatation
+// thread owns (4 and 2; only the requested one when lps_options.theta_rows
+// is set) and every count of resident dilatation / force CTAs per SM (1 up
+// to the occupancy limit) it captures the 12-step CUDA graph the run will
+// replay and times two replays of it from the initial state (the faster of
+// two tries); a choice replaces the default (4 rows, full occupancy) only if
+// it is at least 2 % faster.  None of these changes a result: tiles come from
+// a counter and each cell's arithmetic is the same whichever CTA and thread
+// computes it.  The caller resets the state afterwards.
+int autotune_dense(lps_handle *h, int rows_only) {
+  int max_f = 1, max_t[2] = {1, 1};  // [0]: four rows, [1]: two rows
   for (const auto &gr : h->dg.groups) {
-    max_t = std::max(max_t, gr.max_theta_ctas);
+    max_t[0] = std::max(max_t[0], gr.max_theta_ctas);
+    max_t[1] = std::max(max_t[1], gr.max_theta_ctas2);
     max_f = std::max(max_f, gr.max_force_ctas);
   }
   cudaEvent_t e0, e1;
@@ -806,8 +809,8 @@ int autotune_dense(lps_handle *h) {
     h->graphs.clear();
     h->graph_kernels.clear();
   };
-  auto time_pair = [&](int t, int f, float *ms_out) -> int {
-    dense_set_ctas(h->dg, t, f);
+  auto time_choice = [&](int rows, int t, int f, float *ms_out) -> int {
+    dense_set_ctas(h->dg, rows, t, f);
     drop_graphs();
     cudaGraphExec_t ex;
     int st = get_graph(h, 0, &ex);
@@ -828,27 +831,33 @@ int autotune_dense(lps_handle *h) {
     *ms_out = best;
     return LPS_OK;
   };
+  const int rows0 = rows_only == 2 ? 2 : 4, r0 = rows0 == 4 ? 0 : 1;
   float ref = 0.f;
-  int st = time_pair(max_t, max_f, &ref);
+  int st = time_choice(rows0, max_t[r0], max_f, &ref);
   float best = ref;
-  int best_t = max_t, best_f = max_f;
-  for (int t = 1; t <= max_t && st == LPS_OK; t++)
-    for (int f = 1; f <= max_f && st == LPS_OK; f++) {
-      if (t == max_t && f == max_f) continue;
-      float ms = 0.f;
-      if ((st = time_pair(t, f, &ms))) break;
-      if (ms < best && ms < 0.98f * ref) {
-        best = ms;
-        best_t = t;
-        best_f = f;
+  int best_r = rows0, best_t = max_t[r0], best_f = max_f;
+  for (int rows : {4, 2}) {
+    if (rows_only && rows != rows_only) continue;
+    const int mt = max_t[rows == 4 ? 0 : 1];
+    for (int t = 1; t <= mt && st == LPS_OK; t++)
+      for (int f = 1; f <= max_f && st == LPS_OK; f++) {
+        if (rows == rows0 && t == mt && f == max_f) continue;
+        float ms = 0.f;
+        if ((st = time_choice(rows, t, f, &ms))) break;
+        if (ms < best && ms < 0.98f * ref) {
+          best = ms;
+          best_r = rows;
+          best_t = t;
+          best_f = f;
+        }
       }
-    }
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   drop_graphs();
   if (st == LPS_OK) st = check_device_error(h);
   if (st) return st;
-  dense_set_ctas(h->dg, best_t, best_f);
+  dense_set_ctas(h->dg, best_r, best_t, best_f);
   return LPS_OK;
 }
 
@@ -1065,6 +1074,10 @@ int lps_create(const lps_problem *problems, int n_instances, const lps_options *
   lps_options o;
   if (opt) o = *opt; else lps_default_options(&o);
   if (o.max_horizon <= 1) o.max_horizon = 128;
+  if (o.theta_rows != 0 && o.theta_rows != 2 && o.theta_rows != 4) {
+    g_create_error = "lps_create: theta_rows must be 0, 2 or 4";
+    return LPS_ERR_INVALID_ARG;
+  }
   if (o.precision != LPS_FP64 && o.precision != LPS_FP32_MIXED) {
     g_create_error = "lps_create: precision must be LPS_FP64 or LPS_FP32_MIXED";
     return LPS_ERR_INVALID_ARG;
@@ -1173,7 +1186,8 @@ int lps_create(const lps_problem *problems, int n_instances, const lps_options *
     }
   }
   if ((s = do_reset(h))) return fail(s);
-  if (o.autotune && h->path == LPS_PATH_DENSE && (s = autotune_dense(h))) return fail(s);
+  if (h->path == LPS_PATH_DENSE && o.theta_rows == 2) dense_set_ctas(h->dg, 2, 1 << 20, 1 << 20);
+  if (o.autotune && h->path == LPS_PATH_DENSE && (s = autotune_dense(h, o.theta_rows))) return fail(s);
   if (o.autotune && h->path == LPS_PATH_DENSE && (s = do_reset(h))) return fail(s);
   if (cudaStreamSynchronize(h->stream) != cudaSuccess) {
     h->err = std::string("setup kernels failed: ") + cudaGetErrorString(cudaGetLastError());
@@ -1368,6 +1382,7 @@ int lps_get_info(lps_handle *h, int instance, lps_info *info) {
     const DenseGroup &g0 = h->dg.groups[0];
     info->tile_ctas_theta = (g0.grid_theta + n_sm - 1) / n_sm;
     info->tile_ctas_force = (g0.grid_force + n_sm - 1) / n_sm;
+    info->tile_rows_theta = g0.theta_rows;
   }
   return LPS_OK;
 }

@@ -59,7 +59,9 @@ struct DenseGroup {
   int n_tiles;
   int grid_theta;   // persistent grid sizes
   int grid_force;
+  int theta_rows;   // rows of a dilatation thread: 4 or 2
   int max_theta_ctas, max_force_ctas;  // resident CTAs per SM at full occupancy
+  int max_theta_ctas2;                 // the same for the two-row dilatation kernel
   int *sched;       // device tile-scheduler counters (theta: [0..1], force: [2..3])
   DenseMaps maps;
 };
@@ -100,7 +102,7 @@ int dense_encode_maps(DenseGroup &g, int pitch, int total_rows, double2 *const *
 cudaError_t dense_prepare(DenseGeo &dg);
 // Persistent grids of every group at the given resident CTAs per SM (each
 // clamped to 1..the group's occupancy limit).
-void dense_set_ctas(DenseGeo &dg, int theta_ctas, int force_ctas);
+void dense_set_ctas(DenseGeo &dg, int theta_rows, int theta_ctas, int force_ctas);
 
 // FP32-mixed tile kernels (lps_kernels_dense32.cu): shared-memory limits,
 // persistent grids and launches of one group.

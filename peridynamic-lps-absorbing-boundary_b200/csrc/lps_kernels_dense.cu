@@ -93,7 +93,7 @@ cudaError_t upload_dense_constants(int m, double dx, double dy, double delta, cu
 
 // ---------------------------------------------------------------------------
 // Tile compute.  A force thread owns cells (r0, c) and (r0 + 1, c), a
-// dilatation thread kThRows rows of column c; for every pair of opposite
+// dilatation thread K rows of column c; for every pair of opposite
 // offsets (a, b) / (-a, -b) it reads the two staged neighbours of each cell --
 // the row-(r0+1) reads of one offset are the row-r0 reads of the next, so
 // most of them come from registers.
@@ -103,17 +103,17 @@ cudaError_t upload_dense_constants(int m, double dx, double dy, double delta, cu
 // theta, B = 8 mu / m (:857-869).  Masked tiles (near the domain edge) use the
 // same pairs with absent neighbours zeroed: u = A = B = 0 there, and the
 // owned node's own terms are weighted by which side is present.
-// The dilatation thread owns kThRows adjacent rows of one column (the force
-// thread two), so a staged value it loads feeds the pairs of up to kThRows
-// cells; each cell's sums are the same whatever the rows per thread.
-constexpr int kThRows = 4;
-constexpr int kThThreads = kTileRows * kTileCols / kThRows;
+// The dilatation thread owns K adjacent rows of one column (the force thread
+// two), so a staged value it loads feeds the pairs of up to K cells; each
+// cell's sums are the same whatever the rows per thread.  K is 4 or 2, picked
+// per batch (the autotuner's choice; 4 by default); a CTA has th_threads(K)
+// threads.
+constexpr int th_threads(int K) { return kTileRows * kTileCols / K; }
 
-template <int M, bool FULL>
+template <int M, bool FULL, int K>
 __device__ __forceinline__ void theta_tile(const double2 *__restrict__ su, const uint8_t *__restrict__ sty, int r0,
-                                           int c, double th[kThRows]) {
+                                           int c, double th[K]) {
   using R = Region<M>;
-  constexpr int K = kThRows;
   double s0[K], s1[K];
 #pragma unroll
   for (int k = 0; k < K; k++) s0[k] = s1[k] = 0.0;
@@ -192,8 +192,8 @@ __device__ __forceinline__ void force_tile(const double2 *__restrict__ su, const
 
 // ---------------------------------------------------------------------------
 // Predicted displacements -> dilatation, persistent over tiles.
-template <int M>
-__global__ void __launch_bounds__(kThThreads, 4)
+template <int M, int K>
+__global__ void __launch_bounds__(th_threads(K), K == 4 ? 4 : 3)
     k_theta_tma(const __grid_constant__ CUtensorMap map_u, const __grid_constant__ CUtensorMap map_type, Geo g,
                 const DenseTile *__restrict__ tiles, int tile_begin, int n_tiles, StepPtrs p, int pitch,
                 int skip_abc, int *sched, int *err) {
@@ -231,20 +231,20 @@ __global__ void __launch_bounds__(kThThreads, 4)
     const DenseTile t = tiles[tile_begin + tile];
     const double2 *su = reinterpret_cast<const double2 *>(smem + stage * R::THETA_STAGE);
     const uint8_t *sty = reinterpret_cast<const uint8_t *>(smem + stage * R::THETA_STAGE + R::T_TY);
-    const int r0 = kThRows * warp;
+    const int r0 = K * warp;
     // m_i of the owned cells, fetched while the copy lands
     const size_t cell0 = (size_t)(t.row + M + r0) * pitch + t.col + M + lane;
-    double mi[kThRows];
+    double mi[K];
 #pragma unroll
-    for (int k = 0; k < kThRows; k++) mi[k] = g.m[cell0 + (size_t)k * pitch];
+    for (int k = 0; k < K; k++) mi[k] = g.m[cell0 + (size_t)k * pitch];
     if (!mbar_wait_bounded(&bar[stage], (it >> 1) & 1, err)) return;
-    double th[kThRows];
+    double th[K];
     if (t.flags & kTileFull)
-      theta_tile<M, true>(su, sty, r0, lane, th);
+      theta_tile<M, true, K>(su, sty, r0, lane, th);
     else
-      theta_tile<M, false>(su, sty, r0, lane, th);
+      theta_tile<M, false, K>(su, sty, r0, lane, th);
 #pragma unroll
-    for (int k = 0; k < kThRows; k++) {
+    for (int k = 0; k < K; k++) {
       const uint8_t ty = sty[(r0 + k + M) * R::RT + lane + M];
       if (!(ty & kExists)) continue;
       if (skip_abc && (ty & kActiveAbc)) continue;  // the G_theta kernel writes it
@@ -629,27 +629,36 @@ __global__ void __launch_bounds__(256) k_dense_reset_predict(Geo g, const double
 template <int M>
 static cudaError_t prepare_m(DenseGroup &gr, int n_sm) {
   cudaError_t e;
-  if ((e = cudaFuncSetAttribute(k_theta_tma<M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  if ((e = cudaFuncSetAttribute(k_theta_tma<M, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                Region<M>::THETA_SMEM)) ||
+      (e = cudaFuncSetAttribute(k_theta_tma<M, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 Region<M>::THETA_SMEM)))
     return e;
   if ((e = cudaFuncSetAttribute(k_force_tma<M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 Region<M>::FORCE_SMEM)))
     return e;
-  if ((e = cudaFuncSetAttribute(k_theta_tma<M>, cudaFuncAttributePreferredSharedMemoryCarveout,
+  if ((e = cudaFuncSetAttribute(k_theta_tma<M, 4>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                cudaSharedmemCarveoutMaxShared)) ||
+      (e = cudaFuncSetAttribute(k_theta_tma<M, 2>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                 cudaSharedmemCarveoutMaxShared)) ||
       (e = cudaFuncSetAttribute(k_force_tma<M>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                 cudaSharedmemCarveoutMaxShared)))
     return e;
-  int bt = 0, bf = 0;
-  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, k_theta_tma<M>, kThThreads, Region<M>::THETA_SMEM)))
+  int bt = 0, bt2 = 0, bf = 0;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, k_theta_tma<M, 4>, th_threads(4),
+                                                         Region<M>::THETA_SMEM)) ||
+      (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt2, k_theta_tma<M, 2>, th_threads(2),
+                                                         Region<M>::THETA_SMEM)))
     return e;
   if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf, k_force_tma<M>, kTileThreads, Region<M>::FORCE_SMEM)))
     return e;
   bt = std::max(bt, 1);
   bf = std::max(bf, 1);
+  gr.theta_rows = 4;
   gr.grid_theta = std::min(gr.n_tiles, bt * n_sm);
   gr.grid_force = std::min(gr.n_tiles, bf * n_sm);
   gr.max_theta_ctas = bt;
+  gr.max_theta_ctas2 = std::max(bt2, 1);
   gr.max_force_ctas = bf;
   return cudaSuccess;
 }
@@ -659,12 +668,13 @@ static void prepare_dispatch(DenseGroup &gr, int n_sm, cudaError_t *e) {
   *e = prepare_m<M>(gr, n_sm);
 }
 
-void dense_set_ctas(DenseGeo &dg, int theta_ctas, int force_ctas) {
+void dense_set_ctas(DenseGeo &dg, int theta_rows, int theta_ctas, int force_ctas) {
   int dev = 0, n_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
   for (auto &gr : dg.groups) {
-    const int t = std::max(1, std::min(theta_ctas, gr.max_theta_ctas));
+    gr.theta_rows = theta_rows == 2 ? 2 : 4;
+    const int t = std::max(1, std::min(theta_ctas, gr.theta_rows == 2 ? gr.max_theta_ctas2 : gr.max_theta_ctas));
     const int f = std::max(1, std::min(force_ctas, gr.max_force_ctas));
     gr.grid_theta = std::min(gr.n_tiles, t * n_sm);
     gr.grid_force = std::min(gr.n_tiles, f * n_sm);
@@ -748,12 +758,12 @@ int dense_encode_maps(DenseGroup &g, int pitch, int total_rows, double2 *const *
   return LPS_OK;
 }
 
-template <int M>
-static void launch_theta_group(const DenseGroup &gr, const LaunchGeo &lg, const DenseGeo &dg, const StepPtrs &p,
-                               int ring_u, bool skip_abc, cudaStream_t st) {
+template <int M, int K>
+static void launch_theta_k(const DenseGroup &gr, const LaunchGeo &lg, const DenseGeo &dg, const StepPtrs &p,
+                           int ring_u, bool skip_abc, cudaStream_t st) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(gr.grid_theta);
-  cfg.blockDim = dim3(kThThreads);
+  cfg.blockDim = dim3(th_threads(K));
   cfg.dynamicSmemBytes = Region<M>::THETA_SMEM;
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
@@ -761,8 +771,17 @@ static void launch_theta_group(const DenseGroup &gr, const LaunchGeo &lg, const 
   attr[0].val.priority = dg.tile_priority;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  cudaLaunchKernelEx(&cfg, k_theta_tma<M>, gr.maps.u[ring_u], gr.maps.type, lg.geo, dg.tiles, gr.tile_begin,
+  cudaLaunchKernelEx(&cfg, k_theta_tma<M, K>, gr.maps.u[ring_u], gr.maps.type, lg.geo, dg.tiles, gr.tile_begin,
                      gr.n_tiles, p, dg.pitch, skip_abc ? 1 : 0, gr.sched, dg.d_err);
+}
+
+template <int M>
+static void launch_theta_group(const DenseGroup &gr, const LaunchGeo &lg, const DenseGeo &dg, const StepPtrs &p,
+                               int ring_u, bool skip_abc, cudaStream_t st) {
+  if (gr.theta_rows == 2)
+    launch_theta_k<M, 2>(gr, lg, dg, p, ring_u, skip_abc, st);
+  else
+    launch_theta_k<M, 4>(gr, lg, dg, p, ring_u, skip_abc, st);
 }
 
 template <int M>

@@ -88,19 +88,18 @@ __device__ __forceinline__ void kahan_add(float &s, float &c, float x) {
   s = t;
 }
 
-// Thread owns cells (r0, c) and (r0 + 1, c), as in the FP64 form.  The x and
-// y parts of a bond pair's displacement difference and of the column's
-// partial sums travel together in paired FP32 instructions.
-// The dilatation thread owns kTh32Rows adjacent rows of one column, so a
-// staged value it loads feeds the pairs of up to kTh32Rows cells.
-constexpr int kTh32Rows = 4;
-constexpr int kTh32Threads = kTileRows * kTileCols / kTh32Rows;
+// The dilatation thread owns K (4 or 2) adjacent rows of one column, so a
+// staged value it loads feeds the pairs of up to K cells; each cell's sums
+// are the same whatever K.  The x and y parts of a bond pair's displacement
+// difference and of the column's partial sums travel together in paired FP32
+// instructions.  The force thread owns cells (r0, c) and (r0 + 1, c), as in
+// the FP64 form.
+constexpr int th32_threads(int K) { return kTileRows * kTileCols / K; }
 
-template <int M, bool FULL>
+template <int M, bool FULL, int K>
 __device__ __forceinline__ void theta_tile32(const float2 *__restrict__ su, const uint8_t *__restrict__ sty, int r0,
-                                             int c, float th[kTh32Rows]) {
+                                             int c, float th[K]) {
   using R = Region32<M>;
-  constexpr int K = kTh32Rows;
   const f32x2 *__restrict__ sp = reinterpret_cast<const f32x2 *>(su);
   f32x2 ui[K], part[K];  // own displacement; (x, y) partial sums of the column
   float S[K], C[K];
@@ -201,8 +200,8 @@ __device__ __forceinline__ void force_tile32(const float2 *__restrict__ su, cons
 
 // ---------------------------------------------------------------------------
 // Predicted displacements (FP32 copy) -> dilatation, persistent over tiles.
-template <int M>
-__global__ void __launch_bounds__(kTh32Threads, 6)
+template <int M, int K>
+__global__ void __launch_bounds__(th32_threads(K), K == 4 ? 6 : 4)
     k_theta32(const __grid_constant__ CUtensorMap map_u, const __grid_constant__ CUtensorMap map_type, Geo g,
               const DenseTile *__restrict__ tiles, int tile_begin, int n_tiles, StepPtrs p, int pitch, int skip_abc,
               int *sched, int *err) {
@@ -239,20 +238,20 @@ __global__ void __launch_bounds__(kTh32Threads, 6)
     const InstParams &P = c_inst[t.inst];
     const float2 *su = reinterpret_cast<const float2 *>(smem + stage * R::THETA_STAGE);
     const uint8_t *sty = reinterpret_cast<const uint8_t *>(smem + stage * R::THETA_STAGE + R::T_TY);
-    const int r0 = kTh32Rows * warp;
+    const int r0 = K * warp;
     const size_t cell0 = (size_t)(t.row + M + r0) * pitch + t.col + M + lane;
-    double mi[kTh32Rows];
+    double mi[K];
 #pragma unroll
-    for (int k = 0; k < kTh32Rows; k++) mi[k] = g.m[cell0 + (size_t)k * pitch];
+    for (int k = 0; k < K; k++) mi[k] = g.m[cell0 + (size_t)k * pitch];
     if (!mbar_wait_bounded(&bar[stage], (it >> 1) & 1, err)) return;
-    float th[kTh32Rows];
+    float th[K];
     if (t.flags & kTileFull)
-      theta_tile32<M, true>(su, sty, r0, lane, th);
+      theta_tile32<M, true, K>(su, sty, r0, lane, th);
     else
-      theta_tile32<M, false>(su, sty, r0, lane, th);
+      theta_tile32<M, false, K>(su, sty, r0, lane, th);
     const double scale = 2.0 * P.dx * P.dy * P.dx;
 #pragma unroll
-    for (int k = 0; k < kTh32Rows; k++) {
+    for (int k = 0; k < K; k++) {
       const uint8_t ty = sty[(r0 + k + M) * R::RT + lane + M];
       if (!(ty & kExists)) continue;
       if (skip_abc && (ty & kActiveAbc)) continue;  // the G_theta kernel writes it
@@ -375,26 +374,32 @@ static void prepare32_m(DenseGroup &gr, int n_sm, cudaError_t *out) {
   using R = Region32<M>;
   cudaError_t e;
   *out = cudaSuccess;
-  if ((e = cudaFuncSetAttribute(k_theta32<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, R::THETA_SMEM)) ||
+  if ((e = cudaFuncSetAttribute(k_theta32<M, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, R::THETA_SMEM)) ||
+      (e = cudaFuncSetAttribute(k_theta32<M, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, R::THETA_SMEM)) ||
       (e = cudaFuncSetAttribute(k_force32<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, R::FORCE_SMEM)) ||
-      (e = cudaFuncSetAttribute(k_theta32<M>, cudaFuncAttributePreferredSharedMemoryCarveout,
+      (e = cudaFuncSetAttribute(k_theta32<M, 4>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                cudaSharedmemCarveoutMaxShared)) ||
+      (e = cudaFuncSetAttribute(k_theta32<M, 2>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                 cudaSharedmemCarveoutMaxShared)) ||
       (e = cudaFuncSetAttribute(k_force32<M>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                 cudaSharedmemCarveoutMaxShared))) {
     *out = e;
     return;
   }
-  int bt = 0, bf = 0;
-  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, k_theta32<M>, kTh32Threads, R::THETA_SMEM)) ||
+  int bt = 0, bt2 = 0, bf = 0;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, k_theta32<M, 4>, th32_threads(4), R::THETA_SMEM)) ||
+      (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt2, k_theta32<M, 2>, th32_threads(2), R::THETA_SMEM)) ||
       (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf, k_force32<M>, kTileThreads, R::FORCE_SMEM))) {
     *out = e;
     return;
   }
   bt = std::max(bt, 1);
   bf = std::max(bf, 1);
+  gr.theta_rows = 4;
   gr.grid_theta = std::min(gr.n_tiles, bt * n_sm);
   gr.grid_force = std::min(gr.n_tiles, bf * n_sm);
   gr.max_theta_ctas = bt;
+  gr.max_theta_ctas2 = std::max(bt2, 1);
   gr.max_force_ctas = bf;
 }
 
@@ -404,12 +409,12 @@ cudaError_t dense32_prepare_group(DenseGroup &gr, int n_sm) {
   return e;
 }
 
-template <int M>
-static void theta32_m(const DenseGroup &gr, const LaunchGeo &lg, const DenseGeo &dg, const StepPtrs &p,
+template <int M, int K>
+static void theta32_k(const DenseGroup &gr, const LaunchGeo &lg, const DenseGeo &dg, const StepPtrs &p,
                       int ring_u, bool skip_abc, cudaStream_t st) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(gr.grid_theta);
-  cfg.blockDim = dim3(kTh32Threads);
+  cfg.blockDim = dim3(th32_threads(K));
   cfg.dynamicSmemBytes = Region32<M>::THETA_SMEM;
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
@@ -417,8 +422,17 @@ static void theta32_m(const DenseGroup &gr, const LaunchGeo &lg, const DenseGeo 
   attr[0].val.priority = dg.tile_priority;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  cudaLaunchKernelEx(&cfg, k_theta32<M>, gr.maps.u32[ring_u & 1], gr.maps.type, lg.geo, dg.tiles, gr.tile_begin,
+  cudaLaunchKernelEx(&cfg, k_theta32<M, K>, gr.maps.u32[ring_u & 1], gr.maps.type, lg.geo, dg.tiles, gr.tile_begin,
                      gr.n_tiles, p, dg.pitch, skip_abc ? 1 : 0, gr.sched, dg.d_err);
+}
+
+template <int M>
+static void theta32_m(const DenseGroup &gr, const LaunchGeo &lg, const DenseGeo &dg, const StepPtrs &p,
+                      int ring_u, bool skip_abc, cudaStream_t st) {
+  if (gr.theta_rows == 2)
+    theta32_k<M, 2>(gr, lg, dg, p, ring_u, skip_abc, st);
+  else
+    theta32_k<M, 4>(gr, lg, dg, p, ring_u, skip_abc, st);
 }
 
 template <int M>

@@ -157,8 +157,9 @@ def test_horizon_overflow_is_an_error():
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32_mixed"])
 def test_autotune_changes_no_result(precision):
-    """The autotuner only picks resident CTAs per SM for the tile kernels:
-    every result is the same bits as with the default grids."""
+    """The autotuner only picks rows per dilatation thread and resident CTAs
+    per SM for the tile kernels: every result is the same bits as with the
+    defaults, and so is a run fixed at two rows per dilatation thread."""
     sets = [gen.disc_problem(R=14.0, m=4, nu=0.3, n_steps=40, sigma=3.0),
             gen.disc_problem(R=11.0, m=3, nu=0.2, n_steps=40, sigma=2.5)]
     out = {}
@@ -169,7 +170,13 @@ def test_autotune_changes_no_result(precision):
             info = sv.info(0)
         assert info["path"] == "dense"
         assert 1 <= info["tile_ctas_theta"] <= 8 and 1 <= info["tile_ctas_force"] <= 8
-    for k in range(len(sets)):
-        for key in ("u", "v", "a", "theta"):
-            np.testing.assert_array_equal(out[True][k][1][key], out[False][k][1][key])
-        np.testing.assert_array_equal(out[True][k][0]["E"], out[False][k][0]["E"])
+        assert info["tile_rows_theta"] in (2, 4)
+    with Solver(sets, precision=precision, theta_rows=2) as sv:
+        assert sv.info(0)["tile_rows_theta"] == 2
+        sv.step(40, diag_every=10)
+        out["rows2"] = [(sv.read_diag(k), sv.download(k)) for k in range(len(sets))]
+    for other in (True, "rows2"):
+        for k in range(len(sets)):
+            for key in ("u", "v", "a", "theta"):
+                np.testing.assert_array_equal(out[other][k][1][key], out[False][k][1][key])
+            np.testing.assert_array_equal(out[other][k][0]["E"], out[False][k][0]["E"])
