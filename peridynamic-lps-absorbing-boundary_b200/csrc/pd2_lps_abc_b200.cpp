@@ -21,7 +21,9 @@
 //   --precision fp64|fp32_mixed   (default fp64)
 //   --path auto|dense|csr         (default auto)
 //   --device D                    CUDA device ordinal
-//   --autotune                    time the dense tile kernels' CTAs per SM at setup
+//   --autotune                    time the dense tile kernels' rows per dilatation
+//                                 thread and CTAs per SM at setup
+//   --theta-rows 2|4              fix the rows per dilatation thread
 //   --no-vtk                      skip the VTK files (energy/verify only)
 // Input files are read strictly: a file with fewer values than .data1
 // announces is an error (the reference reads short files silently,
@@ -146,6 +148,7 @@ int main(int argc, char **argv) {
     else if (k == "--device") opt.device = std::atoi(next("--device"));
     else if (k == "--no-vtk") write_vtk = false;
     else if (k == "--autotune") opt.autotune = 1;
+    else if (k == "--theta-rows") opt.theta_rows = std::atoi(next("--theta-rows"));
     else if (k == "--precision") {
       const std::string v = next("--precision");
       if (v == "fp64") opt.precision = LPS_FP64;
