@@ -83,3 +83,13 @@ def test_abi_without_device_fails_cleanly():
     with pytest.raises(LpsError) as e:
         Solver(load_inputs("td"))
     assert e.value.status == -9
+
+
+def test_abi_rejects_bad_theta_rows_before_device():
+    """Options are checked before any device call: rows per dilatation
+    thread other than 0 (default), 2 or 4 is LPS_ERR_INVALID_ARG."""
+    from lps_b200.api import LpsError, Solver
+    with pytest.raises(LpsError) as e:
+        Solver(load_inputs("td"), theta_rows=3)
+    assert e.value.status == -1
+    assert "theta_rows" in str(e.value)
