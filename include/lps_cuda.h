@@ -207,12 +207,18 @@ int lps_profile_kernels(lps_handle *h, int n_steps, int diag_every, lps_kernel_t
  * Its scratch is a file-scope device array sized for LPS_NOALLOC_MAX_NODES
  * nodes (about 0.46 MB on every GPU that loads the library, held until the
  * process exits); larger n_nodes is rejected with LPS_ERR_INVALID_ARG and a
- * message in lps_last_error(NULL).  The first call on a device resolves the
- * array's device address (cudaGetSymbolAddress) -- make that first call before
- * any stream capture on the device.  All calls on a device share the array,
- * so calls that overlap on the GPU (different streams, no ordering) race;
- * every call rewrites the slots it reads, so nothing needs clearing.  The call
- * returns without synchronising. */
+ * message in lps_last_error(NULL).  xy, u, v and a are read as 16-byte x/y
+ * pairs and must be 16-byte aligned, theta and out 8-byte aligned; a view
+ * that starts on an odd double is rejected with LPS_ERR_INVALID_ARG before
+ * any launch.  A CUDA error already pending on the calling thread is reported
+ * as LPS_ERR_CUDA and left pending.  The first call on a device (and the
+ * first after its context was destroyed and recreated, e.g. by
+ * cudaDeviceReset) resolves the array's device address (cudaGetSymbolAddress)
+ * -- make that first call before any stream capture on the device.  All calls
+ * on a device share the array, so calls that overlap on the GPU (different
+ * streams, no ordering) race and must be serialised by the caller; every call
+ * rewrites the slots it reads, so nothing needs clearing.  The call returns
+ * without synchronising. */
 #define LPS_NOALLOC_MAX_NODES 1048576
 #define LPS_NOALLOC_OUT 10
 int lps_state_diag_noalloc(int n_nodes, const double *xy, const double *u, const double *v,

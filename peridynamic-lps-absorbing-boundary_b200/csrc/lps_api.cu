@@ -801,9 +801,17 @@ int autotune_dense(lps_handle *h, int rows_only) {
     max_t[1] = std::max(max_t[1], gr.max_theta_ctas2);
     max_f = std::max(max_f, gr.max_force_ctas);
   }
-  cudaEvent_t e0, e1;
-  LPS_CUDA_TRY(h, cudaEventCreate(&e0));
-  LPS_CUDA_TRY(h, cudaEventCreate(&e1));
+  // the two timing events, destroyed on every return path
+  struct EventPair {
+    cudaEvent_t e[2] = {nullptr, nullptr};
+    ~EventPair() {
+      for (cudaEvent_t x : e)
+        if (x) cudaEventDestroy(x);
+    }
+  } ev;
+  LPS_CUDA_TRY(h, cudaEventCreate(&ev.e[0]));
+  LPS_CUDA_TRY(h, cudaEventCreate(&ev.e[1]));
+  cudaEvent_t e0 = ev.e[0], e1 = ev.e[1];
   auto drop_graphs = [h]() {
     for (auto &g : h->graphs) cudaGraphExecDestroy(g.second);
     h->graphs.clear();
@@ -852,8 +860,6 @@ int autotune_dense(lps_handle *h, int rows_only) {
         }
       }
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
   drop_graphs();
   if (st == LPS_OK) st = check_device_error(h);
   if (st) return st;

@@ -11,7 +11,9 @@
 // and writes them to a device buffer the caller passes.  Its only scratch --
 // one partial-sum record per 256-node block -- is the file-scope device array
 // below, so the call itself never allocates.
+#include <cstdint>
 #include <mutex>
+#include <string>
 
 #include "lps_common.cuh"
 #include "lps_cuda.h"
@@ -33,11 +35,35 @@ constexpr int kMaxBlocks = LPS_NOALLOC_MAX_NODES / kBlock;
 // on a device share it, and each call overwrites the slots it uses.
 static __device__ __align__(256) DiagPartial g_partials[kMaxBlocks];
 
-// Device addresses of g_partials, one per device, resolved once with that
-// device current (in host code the symbol name is only a host-side stand-in).
+// Device addresses of g_partials, one per device, resolved with that device
+// current (in host code the symbol name is only a host-side stand-in).  Each
+// address is kept with the context it was resolved in: a context destroyed
+// and recreated (cudaDeviceReset) reloads the module, so the address is
+// resolved again in the new context.
 constexpr int kMaxDevices = 64;
 DiagPartial *g_addr[kMaxDevices] = {};
+void *g_ctx[kMaxDevices] = {};
 std::mutex g_addr_mu;
+
+// The current driver context (cuCtxGetCurrent through the runtime's entry
+// point table, so the library needs no link against libcuda).
+void *current_context() {
+  using Fn = int (*)(void **);
+  static Fn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<Fn>(p);
+  });
+  void *ctx = nullptr;
+  if (fn && fn(&ctx) != 0) ctx = nullptr;
+  return ctx;
+}
+
+bool aligned(const void *p, uintptr_t a) { return (reinterpret_cast<uintptr_t>(p) & (a - 1)) == 0; }
 
 __global__ void __launch_bounds__(kBlock)
     k_state_partials(int n, const double2 *__restrict__ xy, const double2 *__restrict__ u,
@@ -101,22 +127,40 @@ extern "C" int lps_state_diag_noalloc(int n_nodes, const double *xy, const doubl
     lps::set_create_error("lps_state_diag_noalloc: a device pointer is NULL");
     return LPS_ERR_INVALID_ARG;
   }
+  // the kernel reads x/y pairs as 16-byte double2 loads
+  if (!aligned(xy, 16) || !aligned(u, 16) || !aligned(v, 16) || !aligned(a, 16) || !aligned(theta, 8) ||
+      !aligned(out, 8)) {
+    lps::set_create_error("lps_state_diag_noalloc: xy, u, v, a must be 16-byte aligned, theta and out 8-byte");
+    return LPS_ERR_INVALID_ARG;
+  }
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
     lps::set_create_error("lps_state_diag_noalloc: no current CUDA device");
     return LPS_ERR_NO_DEVICE;
   }
+  {
+    // an error the caller left pending is the caller's: report it, keep it
+    const cudaError_t pending = cudaPeekAtLastError();
+    if (pending != cudaSuccess) {
+      lps::set_create_error((std::string("lps_state_diag_noalloc: a CUDA error was pending before the call: ") +
+                             cudaGetErrorString(pending)).c_str());
+      return LPS_ERR_CUDA;
+    }
+  }
   DiagPartial *part = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_addr_mu);
-    if (!g_addr[dev]) {
+    void *ctx = current_context();
+    if (!g_addr[dev] || g_ctx[dev] != ctx) {
       void *p = nullptr;
       const cudaError_t e = cudaGetSymbolAddress(&p, g_partials);
       if (e != cudaSuccess || !p) {
-        lps::set_create_error("lps_state_diag_noalloc: cudaGetSymbolAddress failed");
+        lps::set_create_error((std::string("lps_state_diag_noalloc: cudaGetSymbolAddress failed: ") +
+                               cudaGetErrorString(e)).c_str());
         return LPS_ERR_CUDA;
       }
       g_addr[dev] = static_cast<DiagPartial *>(p);
+      g_ctx[dev] = ctx;
     }
     part = g_addr[dev];
   }
@@ -127,9 +171,14 @@ extern "C" int lps_state_diag_noalloc(int n_nodes, const double *xy, const doubl
                                                reinterpret_cast<const double2 *>(v),
                                                reinterpret_cast<const double2 *>(a), theta, rho, dx, dy, exclude_r,
                                                part);
-  k_state_finish<<<1, kBlock, 0, st>>>(nblocks, part, out);
-  if (cudaGetLastError() != cudaSuccess) {
-    lps::set_create_error("lps_state_diag_noalloc: kernel launch failed");
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) {
+    k_state_finish<<<1, kBlock, 0, st>>>(nblocks, part, out);
+    e = cudaGetLastError();
+  }
+  if (e != cudaSuccess) {
+    lps::set_create_error((std::string("lps_state_diag_noalloc: kernel launch failed: ") + cudaGetErrorString(e))
+                              .c_str());
     return LPS_ERR_CUDA;
   }
   return LPS_OK;

@@ -1,8 +1,8 @@
 #!/usr/bin/env python
 """Regenerate the golden fixtures in tests/golden/ by running the reference.
 
-Needs the read-only reference sources (default /root/reference) and a C++
-compiler; it builds oracle/_ref/ with oracle/Makefile, then:
+Needs the read-only reference sources (--ref, or the LPS_REFERENCE environment
+variable) and a C++ compiler; it builds oracle/_ref/ with oracle/Makefile, then:
 
 * ``td``  -- the reference's own test set (tests/generate_test_data.cpp: R=30,
   dx=0.5, no absorbing layer, 300 steps), solved by the reference solver with
@@ -106,11 +106,14 @@ def save_outputs(path, job, prefix, meta, keep_vtk=()):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("LPS_REFERENCE"),
+                    help="root of the reference project (default: $LPS_REFERENCE)")
     ap.add_argument("--threads", type=int, default=os.cpu_count())
     ap.add_argument("--r10-steps", type=int, default=600)
     ap.add_argument("--r20-steps", type=int, default=1000)
     args = ap.parse_args()
+    if not args.ref or not os.path.isdir(os.path.join(args.ref, "src")):
+        ap.error("give --ref <reference root> or set LPS_REFERENCE")
     make("ref", ref=args.ref)
     for v, defs in VARIANTS.items():
         make("ref-variant", defs=defs, name=v, ref=args.ref)

@@ -78,3 +78,18 @@ def test_noalloc_rejects_oversize_input():
     status = f(big, 1, 1, 1, 1, 1, 1.0, 1.0, 1.0, -1.0, 1, None)
     assert status == -1
     assert b"LPS_NOALLOC_MAX_NODES" in lib.lps_last_error(None)
+
+
+def test_noalloc_rejects_misaligned_views():
+    lib = load_library()
+    f = _bind(lib)
+    # a view that starts on an odd double (8-byte aligned only) is refused
+    # before any launch; the addresses are never dereferenced
+    ok16, odd8 = 4096, 4096 + 8
+    for args in ((odd8, ok16, ok16, ok16), (ok16, odd8, ok16, ok16), (ok16, ok16, odd8, ok16),
+                 (ok16, ok16, ok16, odd8)):
+        status = f(1000, *args, ok16, 1.0, 1.0, 1.0, -1.0, ok16, None)
+        assert status == -1
+        assert b"16-byte aligned" in lib.lps_last_error(None)
+    status = f(1000, ok16, ok16, ok16, ok16, ok16 + 4, 1.0, 1.0, 1.0, -1.0, ok16, None)
+    assert status == -1
