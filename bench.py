@@ -47,14 +47,21 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["poisson7", "example1"], default="poisson7")
-    ap.add_argument("--time-steps", type=int, default=4000)
+    ap.add_argument("--workload", choices=["poisson7", "example1", "large", "uneven64", "horizon8"],
+                    default="poisson7",
+                    help="poisson7: the 7-instance Poisson-ratio batch (the headline); example1, large "
+                         "(12.57 M nodes), uneven64 (64-instance batch), horizon8 (m=8): the other "
+                         "benchmark configurations")
+    ap.add_argument("--time-steps", type=int, default=None,
+                    help="time steps per bench step (default: the configuration's own count)")
     ap.add_argument("--diag-every", type=int, default=30)
     ap.add_argument("--precision", choices=["both", "fp64", "fp32_mixed"], default="both",
                     help="both: the FP32-mixed form is the headline value, the FP64 plain form "
                          "is timed beside it on the same workload")
     ap.add_argument("--path", default="auto")
-    ap.add_argument("--cpu-sample-steps", type=int, default=20)
+    ap.add_argument("--cpu-sample-steps", type=int, default=None,
+                    help="time steps of the CPU sample (default: about 1.2e8 bond-weighted node-steps, "
+                         "10-20 s on 16 host cores)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep full occupancy instead of searching the tile kernels' resident CTAs at "
@@ -62,18 +69,30 @@ def parse():
     return ap.parse_args()
 
 
+WORKLOAD_TEXT = {
+    "poisson7": "Poisson-ratio batch: 7 x Example-1 disc (R=125 mm, dx=0.5 mm, m=4), nu 0.15..0.45",
+    "example1": "Example 1 disc (R=125 mm, dx=0.5 mm, m=4, nu=0.25)",
+    "large": "large single domain (R=500 mm, dx=0.25 mm, m=4, nu=0.30, 12.57 M nodes)",
+    "uneven64": "uneven batch of 64 discs (R 50..250 mm, dx=0.5 mm, m 3..5, seed 20261203)",
+    "horizon8": "large-horizon disc (R=250 mm, dx=0.5 mm, m=8: 224 neighbours, nu=0.40)",
+}
+NEIGHBOURS = {3: 36, 4: 68, 5: 96, 8: 224}
+
+
 def workload_sets(name, n_steps):
-    from lps_b200 import gen
-    nus = NUS if name == "poisson7" else (0.25,)
-    return [gen.disc_problem(R=125.0, dx=0.5, m=4, nu=nu, n_steps=n_steps) for nu in nus]
+    from lps_b200 import configs
+    return configs.build(name, n_steps)
 
 
 def workload_config(name, sets, args):
-    return {"workload": ("Poisson-ratio batch: 7 x Example-1 disc (R=125 mm, dx=0.5 mm, m=4), "
-                         "nu 0.15..0.45" if name == "poisson7" else "Example 1 disc (R=125 mm, dx=0.5, m=4)"),
-            "instances": len(sets), "nodes_per_instance": sets[0].n_nodes,
-            "abc_nodes_per_instance": sets[0].n_abc, "cloud_size": sets[0].max_cloud,
-            "neighbours": 68, "time_steps_per_run": args.time_steps, "diag_every": args.diag_every,
+    nb = sorted({NEIGHBOURS.get(int(round(s.delta / s.dx)), None) for s in sets}, key=str)
+    return {"workload": WORKLOAD_TEXT[name],
+            "instances": len(sets), "nodes": sum(s.n_nodes for s in sets),
+            "nodes_per_instance": sets[0].n_nodes if len(sets) < 8 else [min(s.n_nodes for s in sets),
+                                                                          max(s.n_nodes for s in sets)],
+            "abc_nodes": sum(s.n_abc for s in sets), "cloud_size": max(s.max_cloud for s in sets),
+            "neighbours": nb[0] if len(nb) == 1 else nb, "time_steps_per_run": args.time_steps,
+            "diag_every": args.diag_every,
             "precision": ("fp32_mixed (value), fp64 (beside it)" if args.precision == "both"
                           else args.precision), "path": args.path,
             "l2": "flushed (256 MiB write) before each timed run; working set > L2"}
@@ -85,7 +104,8 @@ def reference_cpu(s, n_steps, threads):
     """Run oracle/_ref/PD2_LPS_ABC_timing on set s for n_steps; returns
     (node_steps_per_s, seconds, kind) or None when the binary is missing."""
     from lps_b200.files import write_input_set
-    binary = os.path.join(ROOT, "oracle", "_ref", "PD2_LPS_ABC_timing")
+    wide = int(round(s.delta / s.dx)) > 5   # m=8: 225 horizon entries need MAX_HORIZON_LENGTH=256
+    binary = os.path.join(ROOT, "oracle", "_ref", "PD2_LPS_ABC_timing256" if wide else "PD2_LPS_ABC_timing")
     if not os.path.exists(binary):
         return None
     work = tempfile.mkdtemp(prefix="lps_ref_")
@@ -115,8 +135,19 @@ def oracle_cpu(s, n_steps, threads):
     """Fallback CPU leg: the C restatement (oracle/liblps_oracle.so)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle_ctypes
-    r = oracle_ctypes.run(s, n_steps=n_steps, substep=10 ** 9, n_threads=threads)
+    r = oracle_ctypes.run(s, n_steps=n_steps, substep=10 ** 9, n_threads=threads, max_horizon=256)
     return s.n_nodes * n_steps / r["elapsed"], r["elapsed"]
+
+
+def cpu_sample(sets, args):
+    """The instance the CPU legs time and their step count: the nu=0.25
+    instance where there is one (else the first), for about 1.2e8
+    neighbour-weighted node-steps unless --cpu-sample-steps is given."""
+    s = next((t for t in sets if abs(t.nu - 0.25) < 1e-12), sets[0])
+    if args.cpu_sample_steps:
+        return s, args.cpu_sample_steps
+    w = NEIGHBOURS.get(int(round(s.delta / s.dx)), 68) / 68.0
+    return s, max(10, int(round(1.2e8 / (s.n_nodes * w))))
 
 
 def cpu_leg(s, n_steps, threads):
@@ -348,18 +379,20 @@ def run_ours(args, rank, world, local_rank, precision, with_cpu=True):
            "data": "synthetic (generated Example-1 geometry; passive averaging ABC operators)",
            "config": workload_config(args.workload, sets, args) | {"parallelism": f"replicas{world}"},
            "e2e": {"value": e2e_value, "unit": "node-steps/s", "h2d_bytes_per_step": h2d,
-                   "d2h_bytes_per_step": d2h},
+                   "d2h_bytes_per_step": d2h,
+                   "excludes": "lps_create (host setup and the one-time upload of geometry and "
+                               "absorbing-boundary operators), as the reference's timer excludes its setup"},
            "gpu_launches": launches, "roofline": roofline, "clocks": clk,
            "kernel_path": info["path"], "tile_ctas": [info["tile_ctas_theta"], info["tile_ctas_force"]],
            "tile_rows_theta": info["tile_rows_theta"],
            "final_dE_rel": final_dE, "_u": final_u}
     if with_cpu and rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        s_cpu = [s for s in sets if abs(s.nu - 0.25) < 1e-12][0] if len(sets) > 1 else sets[0]
-        v, sec, kind = cpu_leg(s_cpu, args.cpu_sample_steps, threads)
+        s_cpu, n_cpu = cpu_sample(sets, args)
+        v, sec, kind = cpu_leg(s_cpu, n_cpu, threads)
         out["cpu_baseline"] = {"value": v, "unit": "node-steps/s", "cores": threads, "kind": kind,
-                               "sample": f"one nu=0.25 instance ({s_cpu.n_nodes} nodes), "
-                                         f"{args.cpu_sample_steps} time steps, output off, {sec:.2f} s"}
+                               "sample": f"one nu={s_cpu.nu:g} instance ({s_cpu.n_nodes} nodes), "
+                                         f"{n_cpu} time steps, output off, {sec:.2f} s"}
     return out
 
 
@@ -367,9 +400,9 @@ def run_reference(args):
     """The reference's CPU solver on the same workload (bounded sample)."""
     threads = os.cpu_count() or 1
     sets = workload_sets(args.workload, args.time_steps)
-    per_step = args.cpu_sample_steps
+    s, per_run = cpu_sample(sets, args)
+    per_step = max(1, per_run // 4)
     n = per_step * (args.warmup + args.steps)
-    s = [t for t in sets if abs(t.nu - 0.25) < 1e-12][0]
     v, sec, kind = cpu_leg(s, n, threads)
     return {"metric": METRIC, "value": v, "unit": "node-steps/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * sec / (args.warmup + args.steps),
@@ -378,13 +411,17 @@ def run_reference(args):
             "config": workload_config(args.workload, sets, args) | {"parallelism": "openmp"},
             "impl": "reference",
             "cpu_baseline": {"value": v, "unit": "node-steps/s", "cores": threads, "kind": kind,
-                             "sample": f"one nu=0.25 instance ({s.n_nodes} nodes), {n} time steps "
+                             "sample": f"one nu={s.nu:g} instance ({s.n_nodes} nodes), {n} time steps "
                                        f"({per_step} per bench step), output off, {sec:.2f} s"},
             "e2e": {"value": v, "unit": "node-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
 def main():
     args = parse()
+    if args.time_steps is None:
+        sys.path.insert(0, PKG)
+        from lps_b200.configs import STEPS
+        args.time_steps = STEPS[args.workload]
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

@@ -144,7 +144,10 @@ int lps_set_initial(lps_handle *h, int instance, const double *u0, const double 
 /* Re-initialises every instance from its stored initial conditions, as
  * src/main.cpp:624-683 does (u^{-1} = v^{-1} = a^0 = 0, theta^0 from u^0,
  * theta^{-1} = 0), sets the step count to 0 and clears the diagnostics logs
- * and E0.  lps_create ends with an implicit reset. */
+ * and E0.  lps_create ends with an implicit reset.  After a device-side wait
+ * timed out (a call returned LPS_ERR_CUDA saying so), the tile kernels do no
+ * work until this call clears the device error flag and the tile-scheduler
+ * counters; the handle then runs again. */
 int lps_reset(lps_handle *h);
 
 /* Enqueues n_steps time steps, src/main.cpp:718-1164 (predictor, dilatation,

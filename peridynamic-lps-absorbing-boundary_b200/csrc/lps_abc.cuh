@@ -21,9 +21,21 @@ __device__ __forceinline__ double beta_dev(double xi, const InstParams &P) {
   return 0.0;
 }
 
-// G_theta at one ABC node per warp, src/main.cpp:795-812.
+// FP32-mixed form: the force pass's per-node coefficients (A', B') =
+// ((lambda_PD / alpha) q theta, q) with q = m_ref / m_i (coef32.x), alpha =
+// 8 mu / m_ref; (0, -1) where m_i <= 0 (the force pass skips such neighbours,
+// src/main.cpp:852).  Written wherever theta is written.
+__device__ __forceinline__ void write_ab32(float2 *ab32, const float2 *coef32, int node, double th,
+                                           const InstParams &P) {
+  const float2 co = coef32[node];
+  ab32[node] = co.y > 0.f ? make_float2((float)(th * P.f32_ab) * co.x, co.y) : make_float2(0.f, -1.f);
+}
+
+// G_theta at one ABC node per warp, src/main.cpp:795-812 (and, in the
+// FP32-mixed form, the node's force coefficients).
 __device__ __forceinline__ void abc_theta_warp(const Abc &ab, int a, const double *__restrict__ th_n,
-                                               const double *__restrict__ th_nm1, double *theta) {
+                                               const double *__restrict__ th_nm1, double *theta,
+                                               float2 *ab32 = nullptr, const float2 *coef32 = nullptr) {
   const int lane = threadIdx.x & 31;
   if (a >= ab.n_abc || !ab.writes[a]) return;
   const int off = ab.cl_off[a], len = ab.cl_len[a];
@@ -42,7 +54,10 @@ __device__ __forceinline__ void abc_theta_warp(const Abc &ab, int a, const doubl
     acc += wb0 * tb0 + wb1 * tb1;
   }
   acc = warp_sum(acc);
-  if (lane == 0) theta[ab.node[a]] = acc;
+  if (lane == 0) {
+    theta[ab.node[a]] = acc;
+    if (ab32) write_ab32(ab32, coef32, ab.node[a], acc, c_inst[ab.inst[a]]);
+  }
 }
 
 // One cloud entry's contribution to the x and y outputs of a 2-level operator.

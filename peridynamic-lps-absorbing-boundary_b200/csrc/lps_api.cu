@@ -61,8 +61,10 @@ struct lps_handle {
   int ring_u = 3;             // displacement ring depth: 3 (CSR path) or 4 (dense path)
   double *TH[3] = {};
   double2 *U0 = nullptr, *V0 = nullptr;
+  bool fp32 = false;          // the FP32-mixed form
   float2 *U32[2] = {};        // FP32-mixed form: FP32 copies of the predicted level, by step parity
-  float2 *coef32 = nullptr;   // FP32-mixed form: (2(l-m)/m_i, 8mu/m_i) as float2
+  float2 *coef32 = nullptr;   // FP32-mixed form: (q, q) with q = m_ref / m_i; (0, -1) where m_i <= 0
+  float2 *AB32 = nullptr;     // FP32-mixed CSR form: force coefficients (A', B'), written with theta
   // diagnostics
   DiagPartial *partials = nullptr;
   DiagRecord *log = nullptr;
@@ -341,6 +343,7 @@ int build_csr(lps_handle *h, const lps_problem *probs) {
   h->n_total = total;
   h->n_abc_total = total_abc;
   std::vector<double2> xy(total, make_double2(0, 0)), coef(total, make_double2(0, -1));
+  std::vector<float2> coef32(total, make_float2(0.f, -1.f));
   std::vector<uint8_t> type(total, 0);
   std::vector<int> abc_of(total, -1), len(total, 0), nbr((size_t)width * total, -1);
   std::vector<double> m(total, 0.0);
@@ -360,8 +363,11 @@ int build_csr(lps_handle *h, const lps_problem *probs) {
       xy[g] = make_double2(p.nodes[2 * i], p.nodes[2 * i + 1]);
       type[g] = kExists | (p.bctypes[2 * i] == 1 ? kBcAbc : 0);
       m[g] = s.m[i];
-      if (s.m[i] > 0.0)  // src/main.cpp:857-863 coefficients, same division
+      if (s.m[i] > 0.0) {  // src/main.cpp:857-863 coefficients, same division
         coef[g] = make_double2(2.0 * (s.lam - s.mu) / s.m[i], 8.0 * s.mu / s.m[i]);
+        const float q = (float)(s.m_ref / s.m[i]);  // FP32-mixed form, as on the dense path
+        coef32[g] = make_float2(q, q);
+      }
       int l = 0;
       for (int j = 1; j < s.hz_len[i]; j++) {
         const int nb = s.hz[(size_t)i * s.row_len + j];
@@ -401,6 +407,7 @@ int build_csr(lps_handle *h, const lps_problem *probs) {
     return s;
   G.xy = d_xy; G.coef = d_coef; G.type = d_type; G.abc_of = d_abc_of; G.len = d_len;
   G.nbr = d_nbr; G.blk_inst = d_blk; G.m = d_m;
+  if (h->fp32 && (s = dev_upload(h, &h->coef32, coef32))) return s;
   if ((s = upload_abc(h, H, total_abc, abc_of))) return s;
   h->lg.n_node_blocks = total / kNodeBlock;
   h->lg.n_abc_blocks = total_abc / kAbcWarpsPerBlock;
@@ -702,6 +709,8 @@ int finish_dense(lps_handle *h) {
   if ((s = dev_alloc(h, &sched, n_sched))) return s;
   LPS_CUDA_TRY(h, cudaMemset(sched, 0, n_sched * sizeof(int)));
   for (size_t g = 0; g < D.groups.size(); g++) D.groups[g].sched = sched + 4 * g;
+  D.sched = sched;
+  D.n_sched = (int)n_sched;
   return LPS_OK;
 }
 
@@ -747,16 +756,26 @@ int enqueue_step(lps_handle *h, int64_t n, bool diag, const Mark *mark = nullptr
   } else {
     launch_predict_csr(h->lg, p, st);
     M("predict_csr");
-    launch_theta_csr(h->lg, p.u_np1, p.th_np1, p.th_n, p.th_nm1, true, st);
-    M("theta_csr");
+    if (h->fp32) {
+      launch_theta_csr32(h->lg, p.u32_np1, p.th_np1, h->AB32, h->coef32, p.th_n, p.th_nm1, st);
+      M("theta_csr32");
+    } else {
+      launch_theta_csr(h->lg, p.u_np1, p.th_np1, p.th_n, p.th_nm1, true, st);
+      M("theta_csr");
+    }
     k += 2;
     if (h->opt.abcs_step != -1 && h->opt.theta_method == 0 && h->lg.abc.n_abc > 0) {
-      launch_theta_idw(h->lg, p.th_np1, st);
+      launch_theta_idw(h->lg, p.th_np1, st, h->AB32, h->coef32);
       M("theta_idw");
       k++;
     }
-    launch_force_csr(h->lg, p, h->d_step, st);
-    M("force_csr");
+    if (h->fp32) {
+      launch_force_csr32(h->lg, p, h->AB32, h->d_step, st);
+      M("force_csr32");
+    } else {
+      launch_force_csr(h->lg, p, h->d_step, st);
+      M("force_csr");
+    }
     k++;
   }
   if (diag) {
@@ -945,6 +964,13 @@ __global__ void k_reset_abc(Abc ab, const double2 *u0, double2 *s) {
 int do_reset(lps_handle *h) {
   cudaStream_t st = h->stream;
   const int n = h->n_total;
+  // a device-side wait that timed out left its flag set and the tile kernels
+  // idle; clear it and the tile-scheduler counters so the handle runs again
+  if (h->path == LPS_PATH_DENSE && h->dg.d_err) {
+    LPS_CUDA_TRY(h, cudaStreamSynchronize(st));
+    LPS_CUDA_TRY(h, cudaMemsetAsync(h->dg.d_err, 0, sizeof(int), st));
+    if (h->dg.sched) LPS_CUDA_TRY(h, cudaMemsetAsync(h->dg.sched, 0, sizeof(int) * h->dg.n_sched, st));
+  }
   k_reset_state<<<(n + 255) / 256, 256, 0, st>>>(n, h->U0, h->V0, h->U[0], h->U[h->ring_u - 1], h->V[0],
                                                   h->V[2], h->A[0], h->TH[2]);
   LPS_CUDA_TRY(h, cudaMemsetAsync(h->TH[0], 0, sizeof(double) * n, st));
@@ -995,11 +1021,16 @@ int alloc_state(lps_handle *h) {
       (s = dev_alloc(h, &h->U0, n)) || (s = dev_alloc(h, &h->V0, n)))
     return s;
   LPS_CUDA_TRY(h, cudaMemset(h->VH, 0, sizeof(double2) * n));
-  if (h->dg.fp32)
+  if (h->fp32) {
     for (int r = 0; r < 2; r++) {
       if ((s = dev_alloc(h, &h->U32[r], n))) return s;
       LPS_CUDA_TRY(h, cudaMemset(h->U32[r], 0, sizeof(float2) * n));
     }
+    if (h->path == LPS_PATH_CSR) {
+      if ((s = dev_alloc(h, &h->AB32, n))) return s;
+      LPS_CUDA_TRY(h, cudaMemset(h->AB32, 0, sizeof(float2) * n));
+    }
+  }
   // diagnostics partials: node blocks (CSR) or tiles (dense), then ABC blocks
   int n_tiles = 0;
   for (const auto &gr : h->dg.groups) n_tiles = std::max(n_tiles, gr.tile_begin + gr.n_tiles);
@@ -1088,10 +1119,6 @@ int lps_create(const lps_problem *problems, int n_instances, const lps_options *
     g_create_error = "lps_create: precision must be LPS_FP64 or LPS_FP32_MIXED";
     return LPS_ERR_INVALID_ARG;
   }
-  if (o.precision == LPS_FP32_MIXED && o.path == LPS_PATH_CSR) {
-    g_create_error = "lps_create: the FP32-mixed form runs on the dense path only";
-    return LPS_ERR_UNSUPPORTED;
-  }
   if (o.theta_method != 0 && o.theta_method != 1) {
     g_create_error = "lps_create: theta_method must be 0 or 1";
     return LPS_ERR_INVALID_ARG;
@@ -1103,6 +1130,7 @@ int lps_create(const lps_problem *problems, int n_instances, const lps_options *
   }
   lps_handle *h = new lps_handle();
   h->opt = o;
+  h->fp32 = o.precision == LPS_FP32_MIXED;
   h->n_inst = n_instances;
   h->device = o.device;
   auto fail = [&](int s) {
@@ -1152,11 +1180,6 @@ int lps_create(const lps_problem *problems, int n_instances, const lps_options *
   int s = LPS_OK;
   std::vector<Lattice> lat;
   const bool dense_ok = o.path != LPS_PATH_CSR && dense_possible(problems, K, h->setup, lat);
-  if (o.precision == LPS_FP32_MIXED && !dense_ok) {
-    h->err = "lps_create: the FP32-mixed form needs the dense path: every instance an exact dx = dy lattice "
-             "with delta/dx in {2,3,4,5,6,8} and no prenotch";
-    return fail(LPS_ERR_UNSUPPORTED);
-  }
   if (o.path == LPS_PATH_DENSE && !dense_ok) {
     h->err = "lps_create: dense path requested but an instance is not an exact dx = dy lattice "
              "with delta/dx in {2,3,4,5,6,8} and no prenotch";

@@ -76,6 +76,8 @@ struct DenseGeo {
   cudaStream_t side = nullptr;                 // forked stream for the ABC kernels
   cudaEvent_t ev_fork[2] = {nullptr, nullptr}, ev_join[2] = {nullptr, nullptr};
   int *d_err = nullptr;                        // device wait-timeout flag
+  int *sched = nullptr;                        // tile-scheduler counters, 4 per group
+  int n_sched = 0;
   std::vector<std::vector<int>> host_cell_of_node;  // per instance: local node -> global cell
   std::vector<int> host_cells;                      // per instance: cell span
   std::vector<int> host_cell_begin;                 // per instance: first cell

@@ -29,8 +29,17 @@ struct LaunchGeo {
 void launch_predict_csr(const LaunchGeo &g, const StepPtrs &p, cudaStream_t st);
 void launch_theta_csr(const LaunchGeo &g, const double2 *u, double *theta, const double *th_n,
                       const double *th_nm1, bool abc_override, cudaStream_t st);
-void launch_theta_idw(const LaunchGeo &g, double *theta, cudaStream_t st);
+void launch_theta_idw(const LaunchGeo &g, double *theta, cudaStream_t st, float2 *ab32 = nullptr,
+                      const float2 *coef32 = nullptr);
 void launch_force_csr(const LaunchGeo &g, const StepPtrs &p, int *d_step, cudaStream_t st);
+
+// CSR path, FP32-mixed form (lps_kernels_csr32.cu): the predictor above also
+// writes the FP32 copy p.u32_np1; dilatation and force run their bond
+// arithmetic in FP32 from it, with the per-node force coefficients ab32
+// ((lambda_PD / alpha) q theta, q) written beside theta.
+void launch_theta_csr32(const LaunchGeo &g, const float2 *u32, double *theta, float2 *ab32, const float2 *coef32,
+                        const double *th_n, const double *th_nm1, cudaStream_t st);
+void launch_force_csr32(const LaunchGeo &g, const StepPtrs &p, const float2 *ab32, int *d_step, cudaStream_t st);
 
 // Diagnostics: merge the pending ABC displacements into u, then the
 // per-block partial sums and one record per instance.

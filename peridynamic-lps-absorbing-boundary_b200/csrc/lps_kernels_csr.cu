@@ -36,6 +36,7 @@ __global__ void __launch_bounds__(kNodeBlock) k_predict_csr(Geo g, StepPtrs p) {
   up.y = u.y + P.dt * vh.y;
   p.vh[i] = vh;
   p.u_np1[i] = up;
+  if (p.u32_np1) p.u32_np1[i] = make_float2((float)up.x, (float)up.y);  // FP32-mixed form
 }
 
 // Dilatation, src/main.cpp:736-761; ABC blocks (blockIdx >= n_node_blocks)
@@ -76,8 +77,10 @@ __global__ void __launch_bounds__(kNodeBlock)
 
 // Inverse-distance-weighted theta at ABC nodes, src/main.cpp:765-790.  The
 // neighbour lists and weights w = 1/(|r| + 1e-30) are built on the host in the
-// reference's horizon order.  Runs after k_theta_csr (needs current theta).
-__global__ void __launch_bounds__(kNodeBlock) k_theta_idw(Abc ab, double *theta) {
+// reference's horizon order.  Runs after the dilatation pass (needs current
+// theta); in the FP32-mixed form it also writes the nodes' force coefficients.
+__global__ void __launch_bounds__(kNodeBlock)
+    k_theta_idw(Abc ab, double *theta, float2 *ab32, const float2 *coef32) {
   const int a = blockIdx.x * kAbcWarpsPerBlock + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (a >= ab.n_abc || !ab.writes[a]) return;
@@ -91,7 +94,10 @@ __global__ void __launch_bounds__(kNodeBlock) k_theta_idw(Abc ab, double *theta)
   ta = warp_sum(ta);
   ws = warp_sum(ws);
   // every lane has read its neighbours before lane 0 writes (warp_sum syncs)
-  if (lane == 0 && ws > 0.0) theta[ab.node[a]] = ta / ws;
+  if (lane == 0 && ws > 0.0) {
+    theta[ab.node[a]] = ta / ws;
+    if (ab32) write_ab32(ab32, coef32, ab.node[a], ta / ws, c_inst[ab.inst[a]]);
+  }
 }
 
 // Force, src/main.cpp:821-874, with the corrector (:922-925) fused in.  ABC
@@ -221,9 +227,9 @@ void launch_theta_csr(const LaunchGeo &g, const double2 *u, double *theta, const
                                               gth ? 1 : 0);
 }
 
-void launch_theta_idw(const LaunchGeo &g, double *theta, cudaStream_t st) {
+void launch_theta_idw(const LaunchGeo &g, double *theta, cudaStream_t st, float2 *ab32, const float2 *coef32) {
   if (g.abc.n_abc == 0) return;
-  k_theta_idw<<<g.n_abc_blocks, kNodeBlock, 0, st>>>(g.abc, theta);
+  k_theta_idw<<<g.n_abc_blocks, kNodeBlock, 0, st>>>(g.abc, theta, ab32, coef32);
 }
 
 void launch_force_csr(const LaunchGeo &g, const StepPtrs &p, int *d_step, cudaStream_t st) {

@@ -221,7 +221,9 @@ __global__ void __launch_bounds__(th_threads(K), K == 4 ? 4 : 3)
   };
   int tile = s_tile[0];
   if (tid == 0 && tile < n_tiles) issue(0, tile);
-  for (int it = 0; tile < n_tiles; it++, tile = s_tile[it & 1]) {
+  int it = 0;
+  bool failed = false;
+  for (; tile < n_tiles; it++, tile = s_tile[it & 1]) {
     const int stage = it & 1;
     if (tid == 0) {
       const int nx = sched_next(sched);
@@ -237,7 +239,11 @@ __global__ void __launch_bounds__(th_threads(K), K == 4 ? 4 : 3)
     double mi[K];
 #pragma unroll
     for (int k = 0; k < K; k++) mi[k] = g.m[cell0 + (size_t)k * pitch];
-    if (!mbar_wait_bounded(&bar[stage], (it >> 1) & 1, err)) return;
+    const bool landed = mbar_wait_bounded(&bar[stage], (it >> 1) & 1, err);
+    if (__syncthreads_or(!landed)) {  // a copy timed out: leave the loop together
+      failed = true;
+      break;
+    }
     double th[K];
     if (t.flags & kTileFull)
       theta_tile<M, true, K>(su, sty, r0, lane, th);
@@ -253,6 +259,7 @@ __global__ void __launch_bounds__(th_threads(K), K == 4 ? 4 : 3)
     fence_proxy_async_smem();
     __syncthreads();  // the stage is refilled at the start of the next-but-one iteration
   }
+  if (failed && tid == 0) drain_stages(bar, it, s_tile[(it & 1) ^ 1] < n_tiles, err);
   if (tid == 0) sched_finish(sched);
 }
 
@@ -293,7 +300,9 @@ __global__ void __launch_bounds__(kTileThreads, 2)
   };
   int tile = s_tile[0];
   if (tid == 0 && tile < n_tiles) issue(0, tile);
-  for (int it = 0; tile < n_tiles; it++, tile = s_tile[it & 1]) {
+  int it = 0;
+  bool failed = false;
+  for (; tile < n_tiles; it++, tile = s_tile[it & 1]) {
     const int stage = it & 1;
     if (tid == 0) {
       const int nx = sched_next(sched);
@@ -311,7 +320,11 @@ __global__ void __launch_bounds__(kTileThreads, 2)
     // corrector inputs of the owned cells, fetched while the copy lands
     const size_t cell0 = (size_t)(t.row + M + r0) * pitch + t.col + M + lane;
     const double2 vh0 = p.vh[cell0], vh1 = p.vh[cell0 + pitch];
-    if (!mbar_wait_bounded(&bar[stage], (it >> 1) & 1, err)) return;
+    const bool landed = mbar_wait_bounded(&bar[stage], (it >> 1) & 1, err);
+    if (__syncthreads_or(!landed)) {  // a copy timed out: leave the loop together
+      failed = true;
+      break;
+    }
     for (int q = tid; q < R::CELLS; q += kTileThreads) {
       const int rr = q / R::RC, cc = q - rr * R::RC;
       const double2 co = sab[q];
@@ -350,6 +363,7 @@ __global__ void __launch_bounds__(kTileThreads, 2)
     fence_proxy_async_smem();
     __syncthreads();
   }
+  if (failed && tid == 0) drain_stages(bar, it, s_tile[(it & 1) ^ 1] < n_tiles, err);
   if (tid == 0) sched_finish(sched);
 }
 
@@ -582,6 +596,8 @@ __global__ void __launch_bounds__(kTileThreads, 2)
       acc.E += ek + ep;
     }
   }
+  // a copy that timed out may still land: wait it out before the CTA leaves
+  if (!ok && tid == 0) mbar_wait_bounded(bar, 0, err);
   acc.block_reduce_store(partials + tile_begin + blockIdx.x);
 }
 

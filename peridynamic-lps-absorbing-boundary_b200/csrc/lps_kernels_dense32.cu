@@ -227,7 +227,9 @@ __global__ void __launch_bounds__(th32_threads(K), K == 4 ? 6 : 4)
   };
   int tile = s_tile[0];
   if (tid == 0 && tile < n_tiles) issue(0, tile);
-  for (int it = 0; tile < n_tiles; it++, tile = s_tile[it & 1]) {
+  int it = 0;
+  bool failed = false;
+  for (; tile < n_tiles; it++, tile = s_tile[it & 1]) {
     const int stage = it & 1;
     if (tid == 0) {
       const int nx = sched_next(sched);
@@ -243,7 +245,11 @@ __global__ void __launch_bounds__(th32_threads(K), K == 4 ? 6 : 4)
     double mi[K];
 #pragma unroll
     for (int k = 0; k < K; k++) mi[k] = g.m[cell0 + (size_t)k * pitch];
-    if (!mbar_wait_bounded(&bar[stage], (it >> 1) & 1, err)) return;
+    const bool landed = mbar_wait_bounded(&bar[stage], (it >> 1) & 1, err);
+    if (__syncthreads_or(!landed)) {  // a copy timed out: leave the loop together
+      failed = true;
+      break;
+    }
     float th[K];
     if (t.flags & kTileFull)
       theta_tile32<M, true, K>(su, sty, r0, lane, th);
@@ -260,6 +266,7 @@ __global__ void __launch_bounds__(th32_threads(K), K == 4 ? 6 : 4)
     fence_proxy_async_smem();
     __syncthreads();  // the stage is refilled at the start of the next-but-one iteration
   }
+  if (failed && tid == 0) drain_stages(bar, it, s_tile[(it & 1) ^ 1] < n_tiles, err);
   if (tid == 0) sched_finish(sched);
 }
 
@@ -302,7 +309,9 @@ __global__ void __launch_bounds__(kTileThreads, 3)
   };
   int tile = s_tile[0];
   if (tid == 0 && tile < n_tiles) issue(0, tile);
-  for (int it = 0; tile < n_tiles; it++, tile = s_tile[it & 1]) {
+  int it = 0;
+  bool failed = false;
+  for (; tile < n_tiles; it++, tile = s_tile[it & 1]) {
     const int stage = it & 1;
     if (tid == 0) {
       const int nx = sched_next(sched);
@@ -321,7 +330,11 @@ __global__ void __launch_bounds__(kTileThreads, 3)
     // corrector / predictor inputs of the owned cells, fetched while the copy lands
     const double2 vh0 = p.vh[cell0], vh1 = p.vh[cell0 + pitch];
     const double2 un0 = p.u_np1[cell0], un1 = p.u_np1[cell0 + pitch];
-    if (!mbar_wait_bounded(&bar[stage], (it >> 1) & 1, err)) return;
+    const bool landed = mbar_wait_bounded(&bar[stage], (it >> 1) & 1, err);
+    if (__syncthreads_or(!landed)) {  // a copy timed out: leave the loop together
+      failed = true;
+      break;
+    }
     const float dxf = (float)P.dx;
     for (int q = tid; q < R::CELLS; q += kTileThreads) {
       const int rr = q / R::RC, cc = q - rr * R::RC;
@@ -364,6 +377,7 @@ __global__ void __launch_bounds__(kTileThreads, 3)
     fence_proxy_async_smem();
     __syncthreads();
   }
+  if (failed && tid == 0) drain_stages(bar, it, s_tile[(it & 1) ^ 1] < n_tiles, err);
   if (tid == 0) sched_finish(sched);
 }
 

@@ -184,6 +184,17 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
   return false;
 }
 
+// After a timed-out wait in iteration `it` of a double-buffered tile loop:
+// waits (bounded) for the copies still in flight into this CTA's two stages --
+// the one the loop gave up on and, if it was issued, the next one -- so that no
+// bulk copy lands in shared memory after the CTA has left.  Thread 0 (the
+// thread that issued the copies) calls it.
+__device__ __forceinline__ void drain_stages(uint64_t *bar, int it, bool next_issued, int *err) {
+  const int stage = it & 1;
+  mbar_wait_bounded(&bar[stage], (it >> 1) & 1, err);
+  if (next_issued) mbar_wait_bounded(&bar[stage ^ 1], ((it + 1) >> 1) & 1, err);
+}
+
 // Dynamic tile scheduler of the persistent tile kernels: a CTA takes its next
 // tile from a counter, so a CTA that becomes resident late (its SM still runs
 // blocks of the concurrent absorbing-boundary kernel) takes fewer tiles instead

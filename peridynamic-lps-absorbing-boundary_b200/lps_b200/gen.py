@@ -89,11 +89,17 @@ def disc_problem(R: float = 125.0, dx: float = 0.5, m: int = 4, nu: float = 0.25
                  E: float = STEEL_E, rho: float = STEEL_RHO, dt: float = 17.5e-9,
                  n_steps: int = 4000, pulse="baseline", amplitude: float = 1e-3,
                  sigma: float | None = None, centre=(0.0, 0.0), abc: str = "average",
-                 abcs_step: int = 2) -> InputSet:
-    """Build one input set (see the module docstring)."""
+                 abcs_step: int = 2, jitter: float = 0.0, seed: int = 0) -> InputSet:
+    """Build one input set (see the module docstring).  ``jitter`` > 0 moves
+    every node by a seeded uniform offset of up to jitter*dx per coordinate,
+    so the node set is no longer a lattice (horizons then come from the
+    distance search alone, as for an arbitrary node file)."""
     dy = dx
     delta = m * dx
     nodes = disc_lattice(R, dx, dy)
+    if jitter > 0.0:
+        rng = np.random.default_rng(seed)
+        nodes = nodes + rng.uniform(-jitter * dx, jitter * dx, size=nodes.shape)
     N = nodes.shape[0]
     r = np.sqrt(nodes[:, 0] ** 2 + nodes[:, 1] ** 2)
     u0 = np.zeros(2 * N)
