@@ -23,12 +23,17 @@ __device__ __forceinline__ double beta_dev(double xi, const InstParams &P) {
 
 // FP32-mixed form: the force pass's per-node coefficients (A', B') =
 // ((lambda_PD / alpha) q theta, q) with q = m_ref / m_i (coef32.x), alpha =
-// 8 mu / m_ref; (0, -1) where m_i <= 0 (the force pass skips such neighbours,
-// src/main.cpp:852).  Written wherever theta is written.
+// 8 mu / m_ref; the dense path measures bond lengths in lattice units, so its
+// A' carries a factor dx.  Where m_i <= 0: (0, -1) on the CSR path (the force
+// pass skips such neighbours, src/main.cpp:852), (0, 0) on the dense path
+// (such a cell has no neighbours, so it is nobody's neighbour).  Written
+// wherever theta is written.
 __device__ __forceinline__ void write_ab32(float2 *ab32, const float2 *coef32, int node, double th,
                                            const InstParams &P) {
   const float2 co = coef32[node];
-  ab32[node] = co.y > 0.f ? make_float2((float)(th * P.f32_ab) * co.x, co.y) : make_float2(0.f, -1.f);
+  const float l = P.dense ? (float)P.dx : 1.f;
+  ab32[node] = co.y > 0.f ? make_float2((float)(th * P.f32_ab) * co.x * l, co.y)
+                          : make_float2(0.f, P.dense ? 0.f : -1.f);
 }
 
 // G_theta at one ABC node per warp, src/main.cpp:795-812 (and, in the

@@ -619,8 +619,11 @@ int build_dense(lps_handle *h, const lps_problem *probs, const std::vector<Latti
             for (size_t j = 0; j < A.size() && full; j++)
               if (!(type[c + (long)A[j] * P + B[j]] & kExists)) full = false;
           }
-        if (any)
-          tiles.push_back(DenseTile{region_row, region_col, k, full ? kTileFull : 0});
+        if (any) {
+          int flags = full ? kTileFull : 0;
+          if (full && h->fp32 && dense32_tile_deep(M, type, coef32, P, first)) flags |= kTileDeep32;
+          tiles.push_back(DenseTile{region_row, region_col, k, flags});
+        }
       }
   }
   std::stable_sort(tiles.begin(), tiles.end(), [&](const DenseTile &x, const DenseTile &y) {
@@ -665,8 +668,22 @@ int build_dense(lps_handle *h, const lps_problem *probs, const std::vector<Latti
   G.xy = d_xy; G.coef = d_coef; G.type = d_type; G.abc_of = d_abc_of; G.blk_inst = d_blk; G.m = d_m;
   G.len = nullptr; G.nbr = nullptr;
   D.tiles = d_tiles;
-  D.fp32 = h->opt.precision == LPS_FP32_MIXED;
-  if (D.fp32 && (st = dev_upload(h, &h->coef32, coef32))) return st;
+  D.fp32 = h->fp32;
+  if (D.fp32) {
+    // static per-cell corrections of the FP32-mixed tile kernels
+    std::vector<float2> w32(n, make_float2(0.f, 0.f));
+    std::vector<float4> ka32(n, make_float4(0.f, 0.f, 0.f, 0.f));
+    for (int k = 0; k < K; k++)
+      dense32_static(lat[k].M, type, P, D.host_cell_begin[k], D.host_cells[k], w32, ka32);
+    float2 *d_w32;
+    float4 *d_ka32;
+    if ((st = dev_upload(h, &h->coef32, coef32)) || (st = dev_upload(h, &d_w32, w32)) ||
+        (st = dev_upload(h, &d_ka32, ka32)))
+      return st;
+    D.d32.coef32 = h->coef32;
+    D.d32.w32 = d_w32;
+    D.d32.ka32 = d_ka32;
+  }
   if ((st = upload_abc(h, H, total_abc, abc_of))) return st;
   if ((st = upload_abc_sell(h, H))) return st;
   std::map<int, int> done;
@@ -692,7 +709,7 @@ int finish_dense(lps_handle *h) {
   const uint8_t *type = h->lg.geo.type;
   for (auto &gr : D.groups) {
     const int s = dense_encode_maps(gr, D.pitch, D.total_rows, h->U, h->TH, coef, type, D.fp32 ? h->U32 : nullptr,
-                                    h->coef32, h->err);
+                                    h->AB32, h->err);
     if (s) return s;
   }
   LPS_CUDA_TRY(h, cudaStreamCreateWithFlags(&D.side, cudaStreamNonBlocking));
@@ -1026,10 +1043,10 @@ int alloc_state(lps_handle *h) {
       if ((s = dev_alloc(h, &h->U32[r], n))) return s;
       LPS_CUDA_TRY(h, cudaMemset(h->U32[r], 0, sizeof(float2) * n));
     }
-    if (h->path == LPS_PATH_CSR) {
-      if ((s = dev_alloc(h, &h->AB32, n))) return s;
-      LPS_CUDA_TRY(h, cudaMemset(h->AB32, 0, sizeof(float2) * n));
-    }
+    // force coefficients, zero at absent cells (the dense kernels rely on it)
+    if ((s = dev_alloc(h, &h->AB32, n))) return s;
+    LPS_CUDA_TRY(h, cudaMemset(h->AB32, 0, sizeof(float2) * n));
+    h->dg.d32.ab32 = h->AB32;
   }
   // diagnostics partials: node blocks (CSR) or tiles (dense), then ABC blocks
   int n_tiles = 0;

@@ -35,6 +35,15 @@ constexpr int kUring = 4;       // displacement ring depth of the dense path
 
 // tile flags
 constexpr int kTileFull = 1;    // every neighbour of every owned node exists
+constexpr int kTileDeep32 = 2;  // full, and B' = m_ref / m is 1.0f at every owned node and neighbour
+
+// FP32-mixed form: per-cell buffers of the dense kernels.
+struct Dense32 {
+  float2 *ab32;           // force coefficients (A', B'), written with theta; 0 at absent cells
+  const float2 *coef32;   // (q, q) with q = m_ref / m_i; (0, -1) where m_i <= 0
+  const float2 *w32;      // W_i = sum over present offsets of beta (a, b)
+  const float4 *ka32;     // Ka_i = sum over absent offsets of beta xi_hat xi_hat^T: (xx, xy, yy, 0)
+};
 
 struct DenseTile {
   int row;    // global row of the staged region's first row
@@ -50,7 +59,7 @@ struct DenseMaps {
   CUtensorMap coef;       // (2(l-m)/m_i, 8 mu/m_i)
   CUtensorMap type;       // u8 node type
   CUtensorMap u32[2];     // FP32-mixed form: FP32 predicted displacements, by step parity
-  CUtensorMap coef32;     // FP32-mixed form: coef as float2
+  CUtensorMap ab32;       // FP32-mixed form: force coefficients (A', B')
 };
 
 struct DenseGroup {
@@ -73,6 +82,7 @@ struct DenseGeo {
   int total_rows = 0;
   int tile_priority = 0;                       // launch priority of the tile kernels
   bool fp32 = false;                           // FP32-mixed tile kernels
+  Dense32 d32 = {};                            // their per-cell buffers
   cudaStream_t side = nullptr;                 // forked stream for the ABC kernels
   cudaEvent_t ev_fork[2] = {nullptr, nullptr}, ev_join[2] = {nullptr, nullptr};
   int *d_err = nullptr;                        // device wait-timeout flag
@@ -96,10 +106,17 @@ void dense_offsets(int m, std::vector<int> &a, std::vector<int> &b);
 // horizon delta, into __constant__ memory.
 cudaError_t upload_dense_constants(int m, double dx, double dy, double delta, cudaStream_t st);
 // Encodes the TMA descriptors of group g over the given buffers (U32 and
-// coef32 only in the FP32-mixed form, else null).
+// ab32 only in the FP32-mixed form, else null).
 int dense_encode_maps(DenseGroup &g, int pitch, int total_rows, double2 *const *U, double *const *TH,
-                      const double2 *coef, const uint8_t *type, float2 *const *U32, const float2 *coef32,
+                      const double2 *coef, const uint8_t *type, float2 *const *U32, const float2 *ab32,
                       std::string &err);
+// FP32-mixed form, host side: W_i and Ka_i of the existing cells in
+// [first, first + count) of an m-stencil grid, and whether a tile whose first
+// owned cell is first_owned is deep (kTileDeep32).
+void dense32_static(int m, const std::vector<uint8_t> &type, int pitch, long first, long count,
+                    std::vector<float2> &w32, std::vector<float4> &ka32);
+bool dense32_tile_deep(int m, const std::vector<uint8_t> &type, const std::vector<float2> &coef32, int pitch,
+                       long first_owned);
 // Sets shared-memory limits and the persistent grid sizes of each group.
 cudaError_t dense_prepare(DenseGeo &dg);
 // Persistent grids of every group at the given resident CTAs per SM (each

@@ -7,10 +7,11 @@
 //   force       F_i = alpha dV sum_j beta xi_hat [(A'_i + A'_j)|xi| + (B'_i + B'_j) e]  (:821-874)
 // with e = xi_hat . eta, B' = m_ref / m, A' = (lambda_PD / alpha) B' theta and
 // alpha = 8 mu / m_ref, so no material constant enters the FP32 arithmetic.
-// FP32: the bond vector (the FP64 coordinate difference, rounded once), |xi|,
-// beta, the displacement difference (from the FP32 copy of the predicted
-// level) and the sums, which run in chunks of eight bonds added to the node's
-// total with Kahan compensation.  FP64: the state, the Verlet update, theta
+// FP32: the bond vector (the FP64 coordinate difference, rounded once), |xi|
+// and xi_hat (correctly rounded square root and quotients), beta, the
+// displacement difference (from the FP32 copy of the predicted level) and the
+// sums, which run in chunks of eight bonds added to the node's total with
+// Kahan compensation.  FP64: the state, the Verlet update, theta
 // storage, the absorbing-boundary operators (the ABC warps are the FP64
 // form's) and the diagnostics.
 #include "lps_abc.cuh"
@@ -68,7 +69,7 @@ __global__ void __launch_bounds__(kNodeBlock)
       if (j < 0) continue;
       const double2 xj = g.xy[j];
       const float ex = (float)(xj.x - xi_i.x), ey = (float)(xj.y - xi_i.y);
-      const float r = sqrtf(fmaf(ex, ex, ey * ey));
+      const float r = __fsqrt_rn(fmaf(ex, ex, ey * ey));
       const float b = beta32(r, blo, bhi, inv_dx);
       const float2 uj = u32[j];
       const float dot = fmaf(ex, uj.x - ui.x, ey * (uj.y - ui.y));  // xi . eta = |xi| e
@@ -117,10 +118,12 @@ __global__ void __launch_bounds__(kNodeBlock)
         if (abj.y < 0.f) continue;  // m_j <= 0 (:852)
         const double2 xj = g.xy[j];
         const float ex = (float)(xj.x - xi_i.x), ey = (float)(xj.y - xi_i.y);
-        const float r2 = fmaf(ex, ex, ey * ey);
-        const float rinv = rsqrtf(r2);
-        const float r = r2 * rinv;
-        const float hx = ex * rinv, hy = ey * rinv;
+        // correctly rounded square root and quotients: an approximate
+        // reciprocal square root biases every bond's stiffness the same way
+        // each step, and that error grows with the run (about 1e-5 after
+        // 4000 steps of configuration 1)
+        const float r = __fsqrt_rn(fmaf(ex, ex, ey * ey));
+        const float hx = __fdiv_rn(ex, r), hy = __fdiv_rn(ey, r);
         const float b = beta32(r, blo, bhi, inv_dx);
         const float2 uj = u32[j];
         const float e = fmaf(hx, uj.x - ui.x, hy * (uj.y - ui.y));

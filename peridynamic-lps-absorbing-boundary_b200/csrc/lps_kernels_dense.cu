@@ -742,15 +742,14 @@ bool encode(CUtensorMap *map, CUtensorMapDataType dt, size_t elem, const void *b
 
 template <int M>
 void encode_m(DenseGroup &g, int pitch, int rows, double2 *const *U, double *const *TH, const double2 *coef,
-              const uint8_t *type, float2 *const *U32, const float2 *coef32, bool *ok) {
+              const uint8_t *type, float2 *const *U32, const float2 *ab32, bool *ok) {
   using R = Region<M>;
   bool good = true;
   if (U32) {
     for (int r = 0; r < 2; r++)
       good &= encode(&g.maps.u32[r], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, U32[r], 2ull * pitch, rows, 2 * R::RC,
                      R::RR);
-    good &= encode(&g.maps.coef32, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, coef32, 2ull * pitch, rows, 2 * R::RC,
-                   R::RR);
+    good &= encode(&g.maps.ab32, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, ab32, 2ull * pitch, rows, 2 * R::RC, R::RR);
   }
   for (int r = 0; r < kUring; r++)
     good &= encode(&g.maps.u[r], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, U[r], 2ull * pitch, rows, 2 * R::RC, R::RR);
@@ -763,10 +762,10 @@ void encode_m(DenseGroup &g, int pitch, int rows, double2 *const *U, double *con
 }  // namespace
 
 int dense_encode_maps(DenseGroup &g, int pitch, int total_rows, double2 *const *U, double *const *TH,
-                      const double2 *coef, const uint8_t *type, float2 *const *U32, const float2 *coef32,
+                      const double2 *coef, const uint8_t *type, float2 *const *U32, const float2 *ab32,
                       std::string &err) {
   bool ok = false;
-  LPS_DISPATCH_M(g.m, encode_m, g, pitch, total_rows, U, TH, coef, type, U32, coef32, &ok);
+  LPS_DISPATCH_M(g.m, encode_m, g, pitch, total_rows, U, TH, coef, type, U32, ab32, &ok);
   if (!ok) {
     err = "cuTensorMapEncodeTiled failed for the dense layout";
     return LPS_ERR_CUDA;
@@ -835,7 +834,7 @@ int enqueue_dense_step(const DenseGeo &dg, const LaunchGeo &lg, const StepPtrs &
   }
   if (mark) (*mark)("theta_tiles");
   if (abc && lg.theta_method == 0) {
-    launch_theta_idw(lg, p.th_np1, st);
+    launch_theta_idw(lg, p.th_np1, st, dg.fp32 ? dg.d32.ab32 : nullptr, dg.d32.coef32);
     if (mark) (*mark)("theta_idw");
     k++;
   }

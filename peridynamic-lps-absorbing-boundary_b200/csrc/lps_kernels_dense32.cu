@@ -2,11 +2,12 @@
 //
 // Same two persistent passes as the FP64 form (lps_kernels_dense.cu), with
 // the bond arithmetic in FP32:
-//   k_theta32<M>   dilatation (src/main.cpp:736-761) from an FP32 copy of the
-//                  predicted displacements
-//   k_force32<M>   force (:821-874) in FP32; corrector (:922-925) and the next
-//                  predictor (:725-728) in FP64, which also writes the FP32
-//                  copy of the next predicted level
+//   k_theta32<M,K>  dilatation (src/main.cpp:736-761) from an FP32 copy of the
+//                   predicted displacements; its epilogue also writes the force
+//                   pass's per-cell coefficients (A', B') in FP32
+//   k_force32<M>    force (:821-874) in FP32; corrector (:922-925) and the
+//                   next predictor (:725-728) in FP64, which also writes the
+//                   FP32 copy of the next predicted level
 // Kept in FP64: the displacement / velocity / acceleration state and its
 // Verlet update, theta storage, the absorbing-boundary operators (their own
 // kernels are shared with the FP64 form) and the diagnostics.
@@ -18,8 +19,18 @@
 //   F_i     = alpha dx^2 sum beta xi_hat [ (A'+ - A'-) r + (B'_i + B'+) e+ - (B'_i + B'-) e- ]
 // with B' = B / alpha = m_ref / m and A' = dx B' (lambda_PD / alpha) theta,
 // alpha = 8 mu / m_ref: material constants stay out of the FP32 arithmetic.
-// Each stencil column's partial sum is added to the cell's total with Kahan
-// compensation.
+//
+// No per-neighbour existence test.  Absent cells hold u = 0 and A' = B' = 0,
+// so every stencil pair is evaluated the same way, and the terms that an
+// absent neighbour contributes wrongly are removed by two static per-cell
+// quantities, zero at full-horizon cells:
+//   W_i  = sum over present offsets of beta (a, b)
+//   Ka_i = sum over absent offsets of beta xi_hat xi_hat^T
+// -- theta_i gets -W_i . u_i, F_i gets A'_i W_i + B'_i Ka_i u_i.  Tiles whose
+// cells and neighbours all have B' = 1 ("deep" tiles, the interior) use
+//   F_i = sum beta xi_hat [ (A'+ - A'-) r + 2 xi_hat . (u(+) + u(-) - 2 u_i) ],
+// the same sum with the coefficients folded.  Each stencil column's partial
+// sum is added to the cell's total with Kahan compensation.
 #include <cmath>
 
 #include "lps_common.cuh"
@@ -39,22 +50,38 @@ __host__ __device__ constexpr double ct_sqrt(double x) {
 // (a, b) of the unrolled stencil.
 enum StenQ { kHx, kHy, kR, kGx, kGy, kWx, kWy };
 
-__host__ __device__ constexpr float sten_q(int Q, int M, int a, int b) {
+__host__ __device__ constexpr double sten_qd(int Q, int M, int a, int b) {
   const double r = ct_sqrt((double)(a * a + b * b));
   const double beta = r <= M - 0.5 ? 1.0 : (r <= M + 0.5 ? M + 0.5 - r : 0.0);
   switch (Q) {
-    case kHx: return (float)(a / r);           // xi_hat
-    case kHy: return (float)(b / r);
-    case kR: return (float)r;                  // |xi| / dx
-    case kGx: return (float)(beta * a / r);    // beta xi_hat
-    case kGy: return (float)(beta * b / r);
-    case kWx: return (float)(beta * a);        // beta (a, b)
-    default: return (float)(beta * b);
+    case kHx: return a / r;           // xi_hat
+    case kHy: return b / r;
+    case kR: return r;                // |xi| / dx
+    case kGx: return beta * a / r;    // beta xi_hat
+    case kGy: return beta * b / r;
+    case kWx: return beta * a;        // beta (a, b)
+    default: return beta * b;
   }
 }
+__host__ __device__ constexpr float sten_q(int Q, int M, int a, int b) { return (float)sten_qd(Q, M, a, b); }
 
+// Staged-region geometry of the FP32 tile kernels: the dilatation stages the
+// FP32 displacements, the force pass the displacements and (A', B').
 template <int M>
-using Region32 = Region<M, 8, 8>;
+struct Region32 {
+  static constexpr int RR = kTileRows + 2 * M;
+  static constexpr int RC = kTileCols + 2 * M;
+  static constexpr int CELLS = RR * RC;
+  static constexpr int align128(int x) { return (x + 127) / 128 * 128; }
+  static constexpr int U_BYTES = CELLS * 8;
+  static constexpr int THETA_STAGE = align128(U_BYTES);
+  static constexpr int THETA_TX = U_BYTES;
+  static constexpr int F_AB = align128(U_BYTES);
+  static constexpr int FORCE_STAGE = align128(F_AB + CELLS * 8);
+  static constexpr int FORCE_TX = 2 * CELLS * 8;
+  static constexpr int THETA_SMEM = 2 * THETA_STAGE + 64;
+  static constexpr int FORCE_SMEM = 2 * FORCE_STAGE + 64;
+};
 
 // Two FP32 values in one 64-bit register pair, for Blackwell's paired FP32
 // instructions (add/sub/fma .f32x2: one instruction for the x and y parts).
@@ -72,6 +99,11 @@ __device__ __forceinline__ float2 f2_unpack(f32x2 v) {
 __device__ __forceinline__ f32x2 f2_sub(f32x2 a, f32x2 b) {
   f32x2 r;
   asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f32x2 f2_add(f32x2 a, f32x2 b) {
+  f32x2 r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
   return r;
 }
 __device__ __forceinline__ f32x2 f2_fma(f32x2 a, f32x2 b, f32x2 c) {
@@ -92,20 +124,18 @@ __device__ __forceinline__ void kahan_add(float &s, float &c, float x) {
 // staged value it loads feeds the pairs of up to K cells; each cell's sums
 // are the same whatever K.  The x and y parts of a bond pair's displacement
 // difference and of the column's partial sums travel together in paired FP32
-// instructions.  The force thread owns cells (r0, c) and (r0 + 1, c), as in
-// the FP64 form.
+// instructions.  The force thread owns cells (r0, c) and (r0 + 1, c).
 constexpr int th32_threads(int K) { return kTileRows * kTileCols / K; }
 
-template <int M, bool FULL, int K>
-__device__ __forceinline__ void theta_tile32(const float2 *__restrict__ su, const uint8_t *__restrict__ sty, int r0,
-                                             int c, float th[K]) {
-  using R = Region32<M>;
+// sum over pairs of beta (a, b) . (u(+) - u(-)), per owned row; absent cells
+// contribute u = 0 (the -W . u_i correction is applied by the caller).
+template <int M, int K>
+__device__ __forceinline__ void theta_tile32(const float2 *__restrict__ su, int r0, int c, float th[K]) {
   const f32x2 *__restrict__ sp = reinterpret_cast<const f32x2 *>(su);
-  f32x2 ui[K], part[K];  // own displacement; (x, y) partial sums of the column
+  f32x2 part[K];  // (x, y) partial sums of the column
   float S[K], C[K];
 #pragma unroll
   for (int k = 0; k < K; k++) {
-    ui[k] = sp[QI<M>(r0 + k, c)];
     part[k] = 0ull;
     S[k] = C[k] = 0.f;
   }
@@ -116,13 +146,7 @@ __device__ __forceinline__ void theta_tile32(const float2 *__restrict__ su, cons
 #pragma unroll
         for (int k = 0; k < K; k++) {
           const int r = r0 + k;
-          f32x2 d = f2_sub(sp[QI<M>(r + a, c + b)], sp[QI<M>(r - a, c - b)]);
-          if (!FULL) {
-            // absent neighbours hold u = 0; restore the -u_i of the present side
-            const float mp = (sty[(r + a + M) * R::RT + c + b + M] & kExists) ? 1.f : 0.f;
-            const float mm = (sty[(r - a + M) * R::RT + c - b + M] & kExists) ? 1.f : 0.f;
-            d = f2_fma(f2_pack(mm - mp, mm - mp), ui[k], d);
-          }
+          const f32x2 d = f2_sub(sp[QI<M>(r + a, c + b)], sp[QI<M>(r - a, c - b)]);
           part[k] = f2_fma(w, d, part[k]);
         }
       },
@@ -138,19 +162,23 @@ __device__ __forceinline__ void theta_tile32(const float2 *__restrict__ su, cons
   for (int k = 0; k < K; k++) th[k] = S[k] - C[k];
 }
 
-template <int M, bool FULL>
+// Force sums of cells (r0, c), (r0 + 1, c).  DEEP: every coefficient B' is 1
+// (folded form); otherwise the general pair form, whose absent-neighbour terms
+// the caller corrects.
+template <int M, bool DEEP>
 __device__ __forceinline__ void force_tile32(const float2 *__restrict__ su, const float2 *__restrict__ sab, int r0,
                                              int c, float F[2][2]) {
   const f32x2 *__restrict__ sp = reinterpret_cast<const f32x2 *>(su);
   f32x2 ui[2];
-  float2 ab_i[2];
+  float bi[2];
   float S0[2] = {0.f, 0.f}, C0[2] = {0.f, 0.f}, S1[2] = {0.f, 0.f}, C1[2] = {0.f, 0.f};
   float p0[2] = {0.f, 0.f}, p1[2] = {0.f, 0.f};
 #pragma unroll
   for (int k = 0; k < 2; k++) {
     ui[k] = sp[QI<M>(r0 + k, c)];
-    ab_i[k] = sab[QI<M>(r0 + k, c)];
+    bi[k] = sab[QI<M>(r0 + k, c)].y;
   }
+  const f32x2 m2 = f2_pack(-2.f, -2.f);
   for_each_pair<M>(
       [&](auto ac, auto bc) {
         constexpr int a = decltype(ac)::value, b = decltype(bc)::value;
@@ -160,25 +188,22 @@ __device__ __forceinline__ void force_tile32(const float2 *__restrict__ su, cons
         for (int k = 0; k < 2; k++) {
           const int r = r0 + k;
           const int qp = QI<M>(r + a, c + b), qm = QI<M>(r - a, c - b);
-          const float2 abp = sab[qp], abm = sab[qm];
-          const float2 d1 = f2_unpack(f2_sub(sp[qp], ui[k]));  // u(+) - u_i
-          const float2 d2 = f2_unpack(f2_sub(ui[k], sp[qm]));  // u_i - u(-)
-          const float e1 = fmaf(hx, d1.x, hy * d1.y);
-          const float e2 = fmaf(hx, d2.x, hy * d2.y);
-          float T, wp, wm;
-          if (FULL) {
-            T = (abp.x - abm.x) * L;
-            wp = ab_i[k].y + abp.y;
-            wm = ab_i[k].y + abm.y;
+          float T;
+          if (DEEP) {
+            // 2 xi_hat . (u(+) + u(-) - 2 u_i) + (A'+ - A'-) r
+            const float2 s = f2_unpack(f2_fma(m2, ui[k], f2_add(sp[qp], sp[qm])));
+            const float e = fmaf(2.f * hx, s.x, (2.f * hy) * s.y);
+            T = fmaf(L, sab[qp].x - sab[qm].x, e);
           } else {
-            // a valid neighbour has B > 0; an absent one has A = B = 0
-            const float mp = abp.y > 0.f ? 1.f : 0.f, mm = abm.y > 0.f ? 1.f : 0.f;
-            T = fmaf(mp - mm, ab_i[k].x, abp.x - abm.x) * L;
-            wp = fmaf(mp, ab_i[k].y, abp.y);
-            wm = fmaf(mm, ab_i[k].y, abm.y);
+            const float2 abp = sab[qp], abm = sab[qm];
+            const float2 d1 = f2_unpack(f2_sub(sp[qp], ui[k]));  // u(+) - u_i
+            const float2 d2 = f2_unpack(f2_sub(ui[k], sp[qm]));  // u_i - u(-)
+            const float e1 = fmaf(hx, d1.x, hy * d1.y);
+            const float e2 = fmaf(hx, d2.x, hy * d2.y);
+            T = (abp.x - abm.x) * L;
+            T = fmaf(bi[k] + abp.y, e1, T);
+            T = fmaf(-(bi[k] + abm.y), e2, T);
           }
-          T = fmaf(wp, e1, T);
-          T = fmaf(-wm, e2, T);
           p0[k] = fmaf(T, gx, p0[k]);
           p1[k] = fmaf(T, gy, p1[k]);
         }
@@ -199,12 +224,12 @@ __device__ __forceinline__ void force_tile32(const float2 *__restrict__ su, cons
 }
 
 // ---------------------------------------------------------------------------
-// Predicted displacements (FP32 copy) -> dilatation, persistent over tiles.
+// Predicted displacements (FP32 copy) -> dilatation and the force pass's
+// coefficients, persistent over tiles.
 template <int M, int K>
 __global__ void __launch_bounds__(th32_threads(K), K == 4 ? 6 : 4)
-    k_theta32(const __grid_constant__ CUtensorMap map_u, const __grid_constant__ CUtensorMap map_type, Geo g,
-              const DenseTile *__restrict__ tiles, int tile_begin, int n_tiles, StepPtrs p, int pitch, int skip_abc,
-              int *sched, int *err) {
+    k_theta32(const __grid_constant__ CUtensorMap map_u, Geo g, const DenseTile *__restrict__ tiles, int tile_begin,
+              int n_tiles, StepPtrs p, Dense32 d32, int pitch, int skip_abc, int *sched, int *err) {
   using R = Region32<M>;
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t *bar = reinterpret_cast<uint64_t *>(smem + 2 * R::THETA_STAGE);
@@ -220,10 +245,8 @@ __global__ void __launch_bounds__(th32_threads(K), K == 4 ? 6 : 4)
   __syncthreads();
   auto issue = [&](int stage, int tile) {
     const DenseTile t = tiles[tile_begin + tile];
-    unsigned char *base = smem + stage * R::THETA_STAGE;
     mbar_expect_tx(&bar[stage], R::THETA_TX);
-    tma_load_2d(base, &map_u, 2 * t.col, t.row, &bar[stage]);
-    tma_load_2d(base + R::T_TY, &map_type, t.col, t.row, &bar[stage]);
+    tma_load_2d(smem + stage * R::THETA_STAGE, &map_u, 2 * t.col, t.row, &bar[stage]);
   };
   int tile = s_tile[0];
   if (tid == 0 && tile < n_tiles) issue(0, tile);
@@ -239,29 +262,46 @@ __global__ void __launch_bounds__(th32_threads(K), K == 4 ? 6 : 4)
     const DenseTile t = tiles[tile_begin + tile];
     const InstParams &P = c_inst[t.inst];
     const float2 *su = reinterpret_cast<const float2 *>(smem + stage * R::THETA_STAGE);
-    const uint8_t *sty = reinterpret_cast<const uint8_t *>(smem + stage * R::THETA_STAGE + R::T_TY);
     const int r0 = K * warp;
     const size_t cell0 = (size_t)(t.row + M + r0) * pitch + t.col + M + lane;
+    // the owned cells' static data, fetched while the copy lands
     double mi[K];
+    uint8_t ty[K];
+    float q[K];
 #pragma unroll
-    for (int k = 0; k < K; k++) mi[k] = g.m[cell0 + (size_t)k * pitch];
+    for (int k = 0; k < K; k++) {
+      const size_t cell = cell0 + (size_t)k * pitch;
+      mi[k] = g.m[cell];
+      ty[k] = g.type[cell];
+      q[k] = d32.coef32[cell].y;
+    }
     const bool landed = mbar_wait_bounded(&bar[stage], (it >> 1) & 1, err);
     if (__syncthreads_or(!landed)) {  // a copy timed out: leave the loop together
       failed = true;
       break;
     }
     float th[K];
-    if (t.flags & kTileFull)
-      theta_tile32<M, true, K>(su, sty, r0, lane, th);
-    else
-      theta_tile32<M, false, K>(su, sty, r0, lane, th);
+    theta_tile32<M, K>(su, r0, lane, th);
     const double scale = 2.0 * P.dx * P.dy * P.dx;
+    const float dxf = (float)P.dx;
+    const bool full = t.flags & kTileFull;
 #pragma unroll
     for (int k = 0; k < K; k++) {
-      const uint8_t ty = sty[(r0 + k + M) * R::RT + lane + M];
-      if (!(ty & kExists)) continue;
-      if (skip_abc && (ty & kActiveAbc)) continue;  // the G_theta kernel writes it
-      p.th_np1[cell0 + (size_t)k * pitch] = (mi[k] > 0.0) ? (scale / mi[k]) * (double)th[k] : 0.0;
+      if (!(ty[k] & kExists)) continue;
+      const size_t cell = cell0 + (size_t)k * pitch;
+      double thd;
+      if (skip_abc && (ty[k] & kActiveAbc)) {
+        thd = p.th_np1[cell];  // G_theta wrote it a step ahead
+      } else {
+        float tk = th[k];
+        if (!full) {  // absent neighbours: remove their -u_i terms
+          const float2 w = d32.w32[cell], ui = su[QI<M>(r0 + k, lane)];
+          tk -= fmaf(w.x, ui.x, w.y * ui.y);
+        }
+        thd = (mi[k] > 0.0) ? (scale / mi[k]) * (double)tk : 0.0;
+        p.th_np1[cell] = thd;
+      }
+      d32.ab32[cell] = q[k] > 0.f ? make_float2((float)(thd * P.f32_ab) * q[k] * dxf, q[k]) : make_float2(0.f, 0.f);
     }
     fence_proxy_async_smem();
     __syncthreads();  // the stage is refilled at the start of the next-but-one iteration
@@ -272,18 +312,13 @@ __global__ void __launch_bounds__(th32_threads(K), K == 4 ? 6 : 4)
 
 // ---------------------------------------------------------------------------
 // Force (FP32) + corrector + next predictor (FP64), persistent over tiles.
-// The FP32 sum is F / alpha with alpha = 8 mu / m_ref: coef32 holds
-// q = m_ref / m_i for both coefficients, so after the copy lands (theta, coef)
-// become (A', B') = (q (lambda_PD / alpha) theta dx, q) in the coef slot --
-// B' = 1 exactly at full-horizon nodes -- and the per-instance constants are
-// applied once, in FP64, to the finished sum.  Absent neighbours and m <= 0
-// get A' = B' = 0.
+// The FP32 sum is F / alpha with alpha = 8 mu / m_ref; the per-instance
+// constants are applied once, in FP64, to the finished sum.
 template <int M>
 __global__ void __launch_bounds__(kTileThreads, 3)
-    k_force32(const __grid_constant__ CUtensorMap map_u, const __grid_constant__ CUtensorMap map_th,
-              const __grid_constant__ CUtensorMap map_coef, const __grid_constant__ CUtensorMap map_type, Geo g,
-              const DenseTile *__restrict__ tiles, int tile_begin, int n_tiles, StepPtrs p, int pitch, int abc_on,
-              int bump_step, int *d_step, int *sched, int *err) {
+    k_force32(const __grid_constant__ CUtensorMap map_u, const __grid_constant__ CUtensorMap map_ab, Geo g,
+              const DenseTile *__restrict__ tiles, int tile_begin, int n_tiles, StepPtrs p, Dense32 d32, int pitch,
+              int abc_on, int bump_step, int *d_step, int *sched, int *err) {
   using R = Region32<M>;
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t *bar = reinterpret_cast<uint64_t *>(smem + 2 * R::FORCE_STAGE);
@@ -303,9 +338,7 @@ __global__ void __launch_bounds__(kTileThreads, 3)
     unsigned char *base = smem + stage * R::FORCE_STAGE;
     mbar_expect_tx(&bar[stage], R::FORCE_TX);
     tma_load_2d(base, &map_u, 2 * t.col, t.row, &bar[stage]);
-    tma_load_2d(base + R::F_TH, &map_th, t.col, t.row, &bar[stage]);
-    tma_load_2d(base + R::F_CO, &map_coef, 2 * t.col, t.row, &bar[stage]);
-    tma_load_2d(base + R::F_TY, &map_type, t.col, t.row, &bar[stage]);
+    tma_load_2d(base + R::F_AB, &map_ab, 2 * t.col, t.row, &bar[stage]);
   };
   int tile = s_tile[0];
   if (tid == 0 && tile < n_tiles) issue(0, tile);
@@ -322,43 +355,42 @@ __global__ void __launch_bounds__(kTileThreads, 3)
     const InstParams &P = c_inst[t.inst];
     unsigned char *base = smem + stage * R::FORCE_STAGE;
     const float2 *su = reinterpret_cast<const float2 *>(base);
-    const double *sth = reinterpret_cast<const double *>(base + R::F_TH);
-    float2 *sab = reinterpret_cast<float2 *>(base + R::F_CO);
-    const uint8_t *sty = reinterpret_cast<const uint8_t *>(base + R::F_TY);
+    const float2 *sab = reinterpret_cast<const float2 *>(base + R::F_AB);
     const int r0 = 2 * warp;
     const size_t cell0 = (size_t)(t.row + M + r0) * pitch + t.col + M + lane;
     // corrector / predictor inputs of the owned cells, fetched while the copy lands
     const double2 vh0 = p.vh[cell0], vh1 = p.vh[cell0 + pitch];
     const double2 un0 = p.u_np1[cell0], un1 = p.u_np1[cell0 + pitch];
+    const uint8_t ty0 = g.type[cell0], ty1 = g.type[cell0 + pitch];
     const bool landed = mbar_wait_bounded(&bar[stage], (it >> 1) & 1, err);
     if (__syncthreads_or(!landed)) {  // a copy timed out: leave the loop together
       failed = true;
       break;
     }
-    const float dxf = (float)P.dx;
-    for (int q = tid; q < R::CELLS; q += kTileThreads) {
-      const int rr = q / R::RC, cc = q - rr * R::RC;
-      const float2 co = sab[q];
-      const bool valid = (sty[rr * R::RT + cc] & kExists) && co.y >= 0.f;
-      sab[q] = valid ? make_float2(co.x * (float)(sth[q] * P.f32_ab) * dxf, co.y) : make_float2(0.f, 0.f);
-    }
-    __syncthreads();
     float F[2][2];
-    if (t.flags & kTileFull)
+    if (t.flags & kTileDeep32)
       force_tile32<M, true>(su, sab, r0, lane, F);
     else
       force_tile32<M, false>(su, sab, r0, lane, F);
     const double scale = P.f32_b0 * P.dx * P.dy / P.rho;
+    const bool full = t.flags & kTileFull;
 #pragma unroll
     for (int k = 0; k < 2; k++) {
-      const uint8_t ty = sty[(r0 + k + M) * R::RT + lane + M];
+      const uint8_t ty = k == 0 ? ty0 : ty1;
       if (!(ty & kExists)) continue;
       const size_t cell = cell0 + (size_t)k * pitch;
-      const bool valid = sab[QI<M>(r0 + k, lane)].y > 0.f;  // m_i > 0 (:827-831)
+      const float2 abi = sab[QI<M>(r0 + k, lane)];
+      if (!full) {  // absent neighbours: A'_i W_i + B'_i Ka_i u_i
+        const float2 w = d32.w32[cell], ui = su[QI<M>(r0 + k, lane)];
+        const float4 ka = d32.ka32[cell];
+        F[k][0] += fmaf(abi.x, w.x, abi.y * fmaf(ka.x, ui.x, ka.y * ui.y));
+        F[k][1] += fmaf(abi.x, w.y, abi.y * fmaf(ka.y, ui.x, ka.z * ui.y));
+      }
+      const bool valid = abi.y > 0.f;  // m_i > 0 (:827-831)
       const double2 acc =
           valid ? make_double2((double)F[k][0] * scale, (double)F[k][1] * scale) : make_double2(0.0, 0.0);
       p.a_np1[cell] = acc;
-      if (abc_on && (ty & kActiveAbc)) continue;  // G_v writes v; the next theta kernel predicts u
+      if (abc_on && (ty & kActiveAbc)) continue;  // G_v writes v; the end-of-step kernel predicts u
       // corrector (:924) then the next predictor (:727), FP64
       const double2 vh = k == 0 ? vh0 : vh1;
       double2 v, vh2, un;
@@ -383,6 +415,66 @@ __global__ void __launch_bounds__(kTileThreads, 3)
 
 // ---------------------------------------------------------------------------
 // host side
+
+// Static per-cell data of ratio M (see the top of this file): W_i, Ka_i and
+// whether the cell, all its stencil neighbours present, has B' = 1.
+template <int M>
+static void static32_m(const std::vector<uint8_t> &type, int pitch, long first, long count, std::vector<float2> &w32,
+                       std::vector<float4> &ka32) {
+  constexpr Sten<M> sten = make_sten<M>();
+  for (long c = first; c < first + count; c++) {
+    if (!(type[c] & kExists)) continue;
+    double wx = 0, wy = 0, kxx = 0, kxy = 0, kyy = 0;
+    for (int j = 0; j < Sten<M>::N; j++) {
+      const int a = sten.a[j], b = sten.b[j];
+      const long nb = c + (long)a * pitch + b;
+      if (type[nb] & kExists) {
+        wx += sten_qd(kWx, M, a, b);
+        wy += sten_qd(kWy, M, a, b);
+      } else {
+        // beta xi_hat xi_hat^T = g xi_hat^T with g = beta xi_hat
+        const double gx = sten_qd(kGx, M, a, b), gy = sten_qd(kGy, M, a, b);
+        const double hx = sten_qd(kHx, M, a, b), hy = sten_qd(kHy, M, a, b);
+        kxx += gx * hx;
+        kxy += gx * hy;
+        kyy += gy * hy;
+      }
+    }
+    w32[c] = make_float2((float)wx, (float)wy);
+    ka32[c] = make_float4((float)kxx, (float)kxy, (float)kyy, 0.f);
+  }
+}
+
+void dense32_static(int m, const std::vector<uint8_t> &type, int pitch, long first, long count,
+                    std::vector<float2> &w32, std::vector<float4> &ka32) {
+  LPS_DISPATCH_M(m, static32_m, type, pitch, first, count, w32, ka32);
+}
+
+template <int M>
+static void deep32_m(const std::vector<uint8_t> &type, const std::vector<float2> &coef32, int pitch, long first_owned,
+                     bool *deep) {
+  constexpr Sten<M> sten = make_sten<M>();
+  bool ok = true;
+  for (int r = 0; r < kTileRows && ok; r++)
+    for (int q = 0; q < kTileCols && ok; q++) {
+      const long c = first_owned + (long)r * pitch + q;
+      if (!(type[c] & kExists)) continue;
+      if (coef32[c].y != 1.0f) ok = false;
+      for (int j = 0; j < Sten<M>::N && ok; j++) {
+        const long nb = c + (long)sten.a[j] * pitch + sten.b[j];
+        if (!(type[nb] & kExists) || coef32[nb].y != 1.0f) ok = false;
+      }
+    }
+  *deep = ok;
+}
+
+bool dense32_tile_deep(int m, const std::vector<uint8_t> &type, const std::vector<float2> &coef32, int pitch,
+                       long first_owned) {
+  bool deep = false;
+  LPS_DISPATCH_M(m, deep32_m, type, coef32, pitch, first_owned, &deep);
+  return deep;
+}
+
 template <int M>
 static void prepare32_m(DenseGroup &gr, int n_sm, cudaError_t *out) {
   using R = Region32<M>;
@@ -436,8 +528,8 @@ static void theta32_k(const DenseGroup &gr, const LaunchGeo &lg, const DenseGeo 
   attr[0].val.priority = dg.tile_priority;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  cudaLaunchKernelEx(&cfg, k_theta32<M, K>, gr.maps.u32[ring_u & 1], gr.maps.type, lg.geo, dg.tiles, gr.tile_begin,
-                     gr.n_tiles, p, dg.pitch, skip_abc ? 1 : 0, gr.sched, dg.d_err);
+  cudaLaunchKernelEx(&cfg, k_theta32<M, K>, gr.maps.u32[ring_u & 1], lg.geo, dg.tiles, gr.tile_begin, gr.n_tiles, p,
+                     dg.d32, dg.pitch, skip_abc ? 1 : 0, gr.sched, dg.d_err);
 }
 
 template <int M>
@@ -451,10 +543,10 @@ static void theta32_m(const DenseGroup &gr, const LaunchGeo &lg, const DenseGeo 
 
 template <int M>
 static void force32_m(const DenseGroup &gr, const LaunchGeo &lg, const DenseGeo &dg, const StepPtrs &p,
-                      int ring_u, int ring_th, bool abc_on, bool first, int *d_step, cudaStream_t st) {
+                      int ring_u, int, bool abc_on, bool first, int *d_step, cudaStream_t st) {
   k_force32<M><<<gr.grid_force, kTileThreads, Region32<M>::FORCE_SMEM, st>>>(
-      gr.maps.u32[ring_u & 1], gr.maps.th[ring_th], gr.maps.coef32, gr.maps.type, lg.geo, dg.tiles, gr.tile_begin,
-      gr.n_tiles, p, dg.pitch, abc_on ? 1 : 0, first ? 1 : 0, d_step, gr.sched + 2, dg.d_err);
+      gr.maps.u32[ring_u & 1], gr.maps.ab32, lg.geo, dg.tiles, gr.tile_begin, gr.n_tiles, p, dg.d32, dg.pitch,
+      abc_on ? 1 : 0, first ? 1 : 0, d_step, gr.sched + 2, dg.d_err);
 }
 
 void launch_theta32_group(const DenseGroup &gr, const LaunchGeo &lg, const DenseGeo &dg, const StepPtrs &p,
