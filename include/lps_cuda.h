@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define LPS_ABI_VERSION 1
+#define LPS_ABI_VERSION 2
 
 /* status codes */
 #define LPS_OK 0
@@ -96,6 +96,10 @@ typedef struct lps_options {
                             /* occupancy                                      */
   int32_t theta_rows;       /* dense dilatation rows per thread: 0 (default:  */
                             /* 4, or the autotuner's choice), 2 or 4 (fixed)  */
+  int32_t horizon_build;    /* horizon search (src/main.cpp:352-356): 0 auto  */
+                            /* (on the GPU from 50,000 nodes), 1 host bucket  */
+                            /* grid, 2 GPU; both give the same horizons       */
+  int32_t pad;
 } lps_options;
 
 /* One output record: the .energy columns (src/main.cpp:1108-1112), the
@@ -119,6 +123,8 @@ typedef struct lps_info {
                                              /* dilatation / force tiles      */
   int32_t tile_rows_theta, pad2;             /* dense path: rows per thread of */
                                              /* the dilatation tiles          */
+  double horizon_ms;                         /* instance: horizon search time */
+  int32_t horizon_on_gpu, pad3;              /* 1: searched on the GPU        */
 } lps_info;
 
 typedef struct lps_handle lps_handle;

@@ -61,7 +61,7 @@ __device__ __forceinline__ void abc_theta_warp(const Abc &ab, int a, const doubl
   acc = warp_sum(acc);
   if (lane == 0) {
     theta[ab.node[a]] = acc;
-    if (ab32) write_ab32(ab32, coef32, ab.node[a], acc, c_inst[ab.inst[a]]);
+    if (ab32) write_ab32(ab32, coef32, ab.node[a], acc, ab.ip[ab.inst[a]]);
   }
 }
 
@@ -79,7 +79,7 @@ __device__ __forceinline__ void g_entry(const double *__restrict__ g, int len, i
 __device__ __forceinline__ void abc_uv_warp(const Abc &ab, int a, const StepPtrs &p) {
   const int lane = threadIdx.x & 31;
   if (a >= ab.n_abc || !ab.writes[a]) return;
-  const InstParams &P = c_inst[ab.inst[a]];
+  const InstParams &P = ab.ip[ab.inst[a]];
   const int off = ab.cl_off[a], len = ab.cl_len[a];
   const double *__restrict__ gu = ab.gu + 8 * (size_t)off;
   const double *__restrict__ gv = ab.gv + 8 * (size_t)off;

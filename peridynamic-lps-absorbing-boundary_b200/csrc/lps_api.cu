@@ -1120,14 +1120,18 @@ const char *lps_last_error(const lps_handle *h) {
 
 int lps_create(const lps_problem *problems, int n_instances, const lps_options *opt, lps_handle **out) {
   g_create_error.clear();
-  if (!out || !problems || n_instances <= 0 || n_instances > kMaxInstances) {
-    g_create_error = "lps_create: bad arguments (need 1..128 instances and an output pointer)";
+  if (!out || !problems || n_instances <= 0) {
+    g_create_error = "lps_create: bad arguments (need at least one instance and an output pointer)";
     return LPS_ERR_INVALID_ARG;
   }
   *out = nullptr;
   lps_options o;
   if (opt) o = *opt; else lps_default_options(&o);
   if (o.max_horizon <= 1) o.max_horizon = 128;
+  if (o.horizon_build < 0 || o.horizon_build > 2) {
+    g_create_error = "lps_create: horizon_build must be 0, 1 or 2";
+    return LPS_ERR_INVALID_ARG;
+  }
   if (o.theta_rows != 0 && o.theta_rows != 2 && o.theta_rows != 4) {
     g_create_error = "lps_create: theta_rows must be 0, 2 or 4";
     return LPS_ERR_INVALID_ARG;
@@ -1211,10 +1215,12 @@ int lps_create(const lps_problem *problems, int n_instances, const lps_options *
     s = build_csr(h, problems);
   }
   if (s) return fail(s);
-  // per-instance constant table
-  if (upload_inst_params(h->params.data(), K, h->stream) != cudaSuccess) {
-    h->err = "upload of instance constants failed";
-    return fail(LPS_ERR_CUDA);
+  // per-instance constant table: device memory of this handle
+  {
+    InstParams *d_ip = nullptr;
+    if ((s = dev_upload(h, &d_ip, h->params))) return fail(s);
+    h->lg.geo.ip = d_ip;
+    h->lg.abc.ip = d_ip;
   }
   if ((s = alloc_state(h))) return fail(s);
   if (h->path == LPS_PATH_DENSE && (s = finish_dense(h))) return fail(s);
@@ -1430,6 +1436,8 @@ int lps_get_info(lps_handle *h, int instance, lps_info *info) {
     info->tile_ctas_force = (g0.grid_force + n_sm - 1) / n_sm;
     info->tile_rows_theta = g0.theta_rows;
   }
+  info->horizon_ms = s.horizon_ms;
+  info->horizon_on_gpu = s.horizon_on_gpu;
   return LPS_OK;
 }
 

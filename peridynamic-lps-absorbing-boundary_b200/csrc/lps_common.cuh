@@ -6,9 +6,6 @@
 
 namespace lps {
 
-// Per-instance constants (defined in lps_diag.cu, relocatable device code).
-extern __constant__ InstParams c_inst[kMaxInstances];
-
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
@@ -106,12 +103,13 @@ struct DiagAcc {
 
 // Second reduction level: one block per instance folds its node blocks and
 // its ABC blocks (in order) into one record appended to the instance's log.
-void launch_diag_finish(int n_inst, const DiagPartial *partials, int n_node_blocks, DiagRecord *log,
-                        int *log_count, int log_capacity, const int *d_step, cudaStream_t st);
+void launch_diag_finish(const InstParams *ip, int n_inst, const DiagPartial *partials, int n_node_blocks,
+                        DiagRecord *log, int *log_count, int log_capacity, const int *d_step, cudaStream_t st);
 // The same for the dense path's tile partials: instance k folds its tiles
 // [tile_begin, tile_begin + tile_count) and then its ABC blocks, which follow
 // the n_tiles tile partials.
-void launch_diag_finish_tiles(int n_inst, const DiagPartial *partials, int n_tiles, DiagRecord *log,
-                              int *log_count, int log_capacity, const int *d_step, cudaStream_t st);
+void launch_diag_finish_tiles(const InstParams *ip, int n_inst, const DiagPartial *partials, int n_tiles,
+                              DiagRecord *log, int *log_count, int log_capacity, const int *d_step,
+                              cudaStream_t st);
 
 }  // namespace lps

@@ -24,7 +24,6 @@
 
 namespace lps {
 
-constexpr int kMaxInstances = 128;   // entries of the __constant__ table (200 B each)
 constexpr int kNodeBlock = 256;      // threads per node-kernel block
 constexpr int kAbcWarpsPerBlock = 8; // warps per ABC block (one ABC node each)
 
@@ -33,7 +32,8 @@ constexpr uint8_t kExists = 1;       // a real node (not padding)
 constexpr uint8_t kBcAbc = 2;        // BCTypes[2i] == 1 (IDW skips these, :778)
 constexpr uint8_t kActiveAbc = 4;    // overwritten by the G operators this step
 
-// Per-instance constants, in __constant__ memory, indexed by instance id.
+// Per-instance constants, one device table per handle (Geo::ip, Abc::ip),
+// indexed by instance id.
 struct InstParams {
   double dt, half_dt, rho, lam, mu, kappa;
   double c_lm;      // 2 (lambda - mu)      (src/main.cpp:857)
@@ -80,6 +80,7 @@ struct StepPtrs {
 
 // Geometry + static per-node data.
 struct Geo {
+  const InstParams *ip;        // per-instance constants
   int n_total;                 // padded node count
   int ell_width;               // ELL slots
   const double2 *xy;           // coordinates
@@ -94,6 +95,7 @@ struct Geo {
 
 // Packed absorbing-boundary data (all instances).
 struct Abc {
+  const InstParams *ip;        // per-instance constants (the same table as Geo::ip)
   int n_abc;
   const int *node;             // global node index
   const int *inst;             // instance id

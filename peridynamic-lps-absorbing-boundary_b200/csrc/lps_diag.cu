@@ -1,24 +1,18 @@
-// lps_diag.cu -- the per-instance constant table and the second level of the
-// diagnostics reduction (src/main.cpp:986-1062).
+// lps_diag.cu -- the second level of the diagnostics reduction
+// (src/main.cpp:986-1062).
 #include "lps_common.cuh"
 #include "lps_kernels.cuh"
 
 namespace lps {
 
-__constant__ InstParams c_inst[kMaxInstances];
-
-cudaError_t upload_inst_params(const InstParams *p, int n, cudaStream_t st) {
-  return cudaMemcpyToSymbolAsync(c_inst, p, sizeof(InstParams) * n, 0, cudaMemcpyHostToDevice, st);
-}
-
 // One 256-thread block per instance.  Each thread folds a contiguous run of
 // block partials (node blocks, then ABC blocks), then the block folds the
 // threads in order; the result is one DiagRecord appended to the log.
 __global__ void __launch_bounds__(256)
-    k_diag_finish(const DiagPartial *__restrict__ partials, int n_node_blocks, DiagRecord *log,
-                  int *log_count, int log_capacity, const int *d_step) {
+    k_diag_finish(const InstParams *__restrict__ ip, const DiagPartial *__restrict__ partials, int n_node_blocks,
+                  DiagRecord *log, int *log_count, int log_capacity, const int *d_step) {
   const int inst = blockIdx.x;
-  const InstParams &P = c_inst[inst];
+  const InstParams &P = ip[inst];
   const int nb0 = P.node_begin / kNodeBlock;
   const int nb1 = (P.node_begin + P.node_count + kNodeBlock - 1) / kNodeBlock;
   const int ab0 = n_node_blocks + P.abc_begin / kNodeBlock;
@@ -53,10 +47,10 @@ __global__ void __launch_bounds__(256)
 
 // Dense path: the tile partials of instance k, then its ABC blocks.
 __global__ void __launch_bounds__(256)
-    k_diag_finish_tiles(const DiagPartial *__restrict__ partials, int n_tiles, DiagRecord *log, int *log_count,
-                        int log_capacity, const int *d_step) {
+    k_diag_finish_tiles(const InstParams *__restrict__ ip, const DiagPartial *__restrict__ partials, int n_tiles,
+                        DiagRecord *log, int *log_count, int log_capacity, const int *d_step) {
   const int inst = blockIdx.x;
-  const InstParams &P = c_inst[inst];
+  const InstParams &P = ip[inst];
   const int tb = P.tile_begin, n_tb = P.tile_count;
   const int ab0 = n_tiles + P.abc_begin / kNodeBlock;
   const int n_ab = (P.abc_count + kNodeBlock - 1) / kNodeBlock;
@@ -87,14 +81,15 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-void launch_diag_finish_tiles(int n_inst, const DiagPartial *partials, int n_tiles, DiagRecord *log,
-                              int *log_count, int log_capacity, const int *d_step, cudaStream_t st) {
-  k_diag_finish_tiles<<<n_inst, 256, 0, st>>>(partials, n_tiles, log, log_count, log_capacity, d_step);
+void launch_diag_finish_tiles(const InstParams *ip, int n_inst, const DiagPartial *partials, int n_tiles,
+                              DiagRecord *log, int *log_count, int log_capacity, const int *d_step,
+                              cudaStream_t st) {
+  k_diag_finish_tiles<<<n_inst, 256, 0, st>>>(ip, partials, n_tiles, log, log_count, log_capacity, d_step);
 }
 
-void launch_diag_finish(int n_inst, const DiagPartial *partials, int n_node_blocks, DiagRecord *log,
-                        int *log_count, int log_capacity, const int *d_step, cudaStream_t st) {
-  k_diag_finish<<<n_inst, 256, 0, st>>>(partials, n_node_blocks, log, log_count, log_capacity, d_step);
+void launch_diag_finish(const InstParams *ip, int n_inst, const DiagPartial *partials, int n_node_blocks,
+                        DiagRecord *log, int *log_count, int log_capacity, const int *d_step, cudaStream_t st) {
+  k_diag_finish<<<n_inst, 256, 0, st>>>(ip, partials, n_node_blocks, log, log_count, log_capacity, d_step);
 }
 
 }  // namespace lps

@@ -11,9 +11,6 @@ namespace lps {
 // Called after each kernel launch with the kernel's name (per-kernel timing).
 using Mark = std::function<void(const char *)>;
 
-// Uploads the per-instance constant table.
-cudaError_t upload_inst_params(const InstParams *p, int n, cudaStream_t st);
-
 // Step geometry shared by every launch of a handle.
 struct LaunchGeo {
   Geo geo;

@@ -22,7 +22,7 @@ __global__ void __launch_bounds__(kNodeBlock) k_predict_csr(Geo g, StepPtrs p) {
   if (i >= g.n_total) return;
   const uint8_t t = g.type[i];
   if (!(t & kExists)) return;
-  const InstParams &P = c_inst[g.blk_inst[blockIdx.x]];
+  const InstParams &P = g.ip[g.blk_inst[blockIdx.x]];
   double2 u = p.u_n[i];
   if (t & kActiveAbc) {
     u = p.s_abc[g.abc_of[i]];
@@ -56,7 +56,7 @@ __global__ void __launch_bounds__(kNodeBlock)
   const uint8_t t = g.type[i];
   if (!(t & kExists)) return;
   if (g_theta_override && (t & kActiveAbc)) return;  // written by the ABC warps
-  const InstParams &P = c_inst[g.blk_inst[blockIdx.x]];
+  const InstParams &P = g.ip[g.blk_inst[blockIdx.x]];
   const double2 xi_i = g.xy[i], ui = u[i];
   const int len = g.len[i];
   double theta_sum = 0.0;
@@ -96,7 +96,7 @@ __global__ void __launch_bounds__(kNodeBlock)
   // every lane has read its neighbours before lane 0 writes (warp_sum syncs)
   if (lane == 0 && ws > 0.0) {
     theta[ab.node[a]] = ta / ws;
-    if (ab32) write_ab32(ab32, coef32, ab.node[a], ta / ws, c_inst[ab.inst[a]]);
+    if (ab32) write_ab32(ab32, coef32, ab.node[a], ta / ws, ab.ip[ab.inst[a]]);
   }
 }
 
@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(kNodeBlock)
   if (i >= g.n_total) return;
   const uint8_t t = g.type[i];
   if (!(t & kExists)) return;
-  const InstParams &P = c_inst[g.blk_inst[blockIdx.x]];
+  const InstParams &P = g.ip[g.blk_inst[blockIdx.x]];
   const double m_i = g.m[i];
   double2 acc = make_double2(0.0, 0.0);
   if (m_i > 0.0) {
@@ -181,7 +181,7 @@ __global__ void __launch_bounds__(kNodeBlock)
   }
   const int i = blockIdx.x * kNodeBlock + threadIdx.x;
   if (i < g.n_total && (g.type[i] & kExists)) {
-    const InstParams &P = c_inst[g.blk_inst[blockIdx.x]];
+    const InstParams &P = g.ip[g.blk_inst[blockIdx.x]];
     const int local = i - P.node_begin;
     const double2 xy = g.xy[i], un = u[i], vn = v[i], an = a[i];
     const double th = theta[i];
@@ -250,7 +250,7 @@ void launch_diag_csr(const LaunchGeo &g, const double2 *u, const double2 *v, con
   const int abc_blocks = (g.abc.n_abc + kNodeBlock - 1) / kNodeBlock;
   k_diag_csr<<<g.n_node_blocks + abc_blocks, kNodeBlock, 0, st>>>(g.geo, g.abc, u, v, a, theta,
                                                                    partials, g.n_node_blocks);
-  launch_diag_finish(g.n_inst, partials, g.n_node_blocks, log, log_count, log_capacity, d_step, st);
+  launch_diag_finish(g.geo.ip, g.n_inst, partials, g.n_node_blocks, log, log_count, log_capacity, d_step, st);
 }
 
 }  // namespace lps

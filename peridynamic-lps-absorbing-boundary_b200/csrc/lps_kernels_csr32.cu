@@ -56,7 +56,7 @@ __global__ void __launch_bounds__(kNodeBlock)
   const uint8_t t = g.type[i];
   if (!(t & kExists)) return;
   if (g_theta_override && (t & kActiveAbc)) return;  // written by the ABC warps
-  const InstParams &P = c_inst[g.blk_inst[blockIdx.x]];
+  const InstParams &P = g.ip[g.blk_inst[blockIdx.x]];
   const float blo = (float)P.beta_lo, bhi = (float)P.beta_hi, inv_dx = (float)(1.0 / P.dx);
   const double2 xi_i = g.xy[i];
   const float2 ui = u32[i];
@@ -100,7 +100,7 @@ __global__ void __launch_bounds__(kNodeBlock)
   if (i >= g.n_total) return;
   const uint8_t t = g.type[i];
   if (!(t & kExists)) return;
-  const InstParams &P = c_inst[g.blk_inst[blockIdx.x]];
+  const InstParams &P = g.ip[g.blk_inst[blockIdx.x]];
   const float2 abi = ab32[i];
   double2 acc = make_double2(0.0, 0.0);
   if (abi.y > 0.f) {  // m_i > 0 (:827-831)

@@ -310,7 +310,7 @@ __global__ void __launch_bounds__(kTileThreads, 2)
       if (nx < n_tiles) issue(stage ^ 1, nx);
     }
     const DenseTile t = tiles[tile_begin + tile];
-    const InstParams &P = c_inst[t.inst];
+    const InstParams &P = g.ip[t.inst];
     unsigned char *base = smem + stage * R::FORCE_STAGE;
     double2 *su = reinterpret_cast<double2 *>(base);
     const double *sth = reinterpret_cast<const double *>(base + R::F_TH);
@@ -390,7 +390,7 @@ __global__ void __launch_bounds__(32 * kSellWarps) k_abc_sell(Abc ab, StepPtrs p
   const SellSlice sl = ab.slices[blockIdx.x];
   const int a = ab.sell_a[blockIdx.x * 32 + lane];
   const int inst = a >= 0 ? ab.inst[a] : 0;
-  const bool kin = c_inst[inst].kinematic != 0;
+  const bool kin = ab.ip[inst].kinematic != 0;
   const double *__restrict__ g = ab.sell_g + sl.goff + lane;
   const int *__restrict__ ix = ab.sell_idx + sl.ioff + lane;
   double s[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // ux, uy, vx, vy, theta
@@ -434,7 +434,7 @@ __global__ void __launch_bounds__(32 * kSellWarps) k_abc_sell(Abc ab, StepPtrs p
     if (kin) {
       // v = (u^{n+1} - u^n) / dt with this node's u^n, src/main.cpp:940-943
       const double2 un = p.u_n[node];
-      const double dt = c_inst[inst].dt;
+      const double dt = ab.ip[inst].dt;
       p.v_np1[node] = make_double2((s[0] - un.x) / dt, (s[1] - un.y) / dt);
     } else {
       p.v_np1[node] = make_double2(s[2], s[3]);
@@ -456,7 +456,7 @@ __global__ void __launch_bounds__(256) k_abc_predict(Abc ab, StepPtrs p) {
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= ab.n_abc || !ab.writes[a]) return;
   const int node = ab.node[a];
-  const InstParams &P = c_inst[ab.inst[a]];
+  const InstParams &P = ab.ip[ab.inst[a]];
   const double2 u = p.s_abc[a], v = p.v_np1[node], acc = p.a_np1[node];
   double2 vh, up;
   vh.x = v.x + P.half_dt * acc.x;
@@ -499,7 +499,7 @@ __device__ __forceinline__ void theta_cell_into(const Geo &g, const double2 *u, 
 __global__ void __launch_bounds__(256) k_theta_dense_init(Geo g, const double2 *u, double *theta) {
   const size_t cell = (size_t)blockIdx.x * 256 + threadIdx.x;
   if (cell >= (size_t)g.n_total || !(g.type[cell] & kExists)) return;
-  const InstParams &P = c_inst[g.blk_inst[blockIdx.x]];
+  const InstParams &P = g.ip[g.blk_inst[blockIdx.x]];
   double th = 0.0;
   LPS_DISPATCH_M(P.stencil, theta_cell_into, g, u, cell, P.pitch, &th);
   theta[cell] = th;
@@ -534,7 +534,7 @@ __global__ void __launch_bounds__(kTileThreads, 2)
     tma_load_2d(smem, &map_u, 2 * t.col, t.row, bar);
     tma_load_2d(smem + R::T_TY, &map_type, t.col, t.row, bar);
   }
-  const InstParams &P = c_inst[t.inst];
+  const InstParams &P = g.ip[t.inst];
   const int r0 = 2 * warp;
   const size_t cell0 = (size_t)(t.row + M + r0) * pitch + t.col + M + lane;
   // the owned cells' other fields, fetched while the copy lands
@@ -628,7 +628,7 @@ __global__ void __launch_bounds__(256) k_dense_reset_predict(Geo g, const double
     vh[cell] = make_double2(0.0, 0.0);
     return;
   }
-  const InstParams &P = c_inst[g.blk_inst[blockIdx.x]];
+  const InstParams &P = g.ip[g.blk_inst[blockIdx.x]];
   const double2 u = u0[cell], v = v0[cell];
   double2 h, up;
   h.x = v.x + P.half_dt * 0.0;
@@ -906,7 +906,7 @@ void launch_diag_dense(const DenseGeo &dg, const LaunchGeo &lg, int ring_u, cons
   }
   const int abc_blocks = (lg.abc.n_abc + kNodeBlock - 1) / kNodeBlock;
   if (abc_blocks > 0) k_diag_abc<<<abc_blocks, kNodeBlock, 0, st>>>(lg.abc, u, v, partials + n_tiles);
-  launch_diag_finish_tiles(lg.n_inst, partials, n_tiles, log, log_count, log_capacity, d_step, st);
+  launch_diag_finish_tiles(lg.geo.ip, lg.n_inst, partials, n_tiles, log, log_count, log_capacity, d_step, st);
 }
 
 }  // namespace lps

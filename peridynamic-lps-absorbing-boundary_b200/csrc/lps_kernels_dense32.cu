@@ -260,7 +260,7 @@ __global__ void __launch_bounds__(th32_threads(K), K == 4 ? 6 : 4)
       if (nx < n_tiles) issue(stage ^ 1, nx);
     }
     const DenseTile t = tiles[tile_begin + tile];
-    const InstParams &P = c_inst[t.inst];
+    const InstParams &P = g.ip[t.inst];
     const float2 *su = reinterpret_cast<const float2 *>(smem + stage * R::THETA_STAGE);
     const int r0 = K * warp;
     const size_t cell0 = (size_t)(t.row + M + r0) * pitch + t.col + M + lane;
@@ -352,7 +352,7 @@ __global__ void __launch_bounds__(kTileThreads, 3)
       if (nx < n_tiles) issue(stage ^ 1, nx);
     }
     const DenseTile t = tiles[tile_begin + tile];
-    const InstParams &P = c_inst[t.inst];
+    const InstParams &P = g.ip[t.inst];
     unsigned char *base = smem + stage * R::FORCE_STAGE;
     const float2 *su = reinterpret_cast<const float2 *>(base);
     const float2 *sab = reinterpret_cast<const float2 *>(base + R::F_AB);

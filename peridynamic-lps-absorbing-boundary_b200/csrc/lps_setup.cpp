@@ -7,6 +7,7 @@
 #include "lps_setup.h"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <limits>
@@ -164,7 +165,15 @@ int setup_instance(const lps_problem &p, const lps_options &o, InstanceSetup &s,
   s.row_len = o.max_horizon > 0 ? o.max_horizon : 128;
   {
     const double horizon_search_r = R + dx / 2.0 + 1e-5;
-    const int r = build_horizons(N, p.nodes, horizon_search_r, s.row_len, s.hz_len, s.hz);
+    s.horizon_on_gpu = o.horizon_build == 2 || (o.horizon_build == 0 && N >= 50000);
+    const auto t0 = std::chrono::steady_clock::now();
+    const int r = s.horizon_on_gpu ? build_horizons_gpu(N, p.nodes, horizon_search_r, s.row_len, s.hz_len, s.hz)
+                                   : build_horizons(N, p.nodes, horizon_search_r, s.row_len, s.hz_len, s.hz);
+    s.horizon_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    if (r == LPS_ERR_CUDA) {
+      err = "lps_create: the horizon search on the GPU failed";
+      return r;
+    }
     if (r < 0) {
       err = "found_node_no > max_node_no; increase max_node_no.";
       return r;

@@ -16,6 +16,8 @@ struct InstanceSetup {
   double dt_lps = 0;                       // :555-581 (sampled, informational)
   int n_corrected = 0;                     // :473-475
   int max_len = 0;                         // longest horizon incl. self
+  double horizon_ms = 0;                   // wall time of the horizon search
+  int horizon_on_gpu = 0;                  // 1: lps_horizons.cu did it
   int row_len = 0;                         // columns of hz (the max_horizon option)
   std::vector<int> hz_len;                 // [n] horizon length incl. self
   std::vector<int> hz;                     // [n][row_len], col 0 = self, -1 padded
@@ -34,5 +36,9 @@ int setup_instance(const lps_problem &p, const lps_options &o, InstanceSetup &s,
 // Returns the longest row, or LPS_ERR_HORIZON if a row exceeds row_len.
 int build_horizons(int n, const double *xy, double r, int row_len, std::vector<int> &len,
                    std::vector<int> &hz);
+// The same search on the current CUDA device (lps_horizons.cu); the same
+// result, or LPS_ERR_CUDA.
+int build_horizons_gpu(int n, const double *xy, double r, int row_len, std::vector<int> &len,
+                       std::vector<int> &hz);
 
 }  // namespace lps

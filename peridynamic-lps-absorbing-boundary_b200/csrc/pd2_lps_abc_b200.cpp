@@ -25,20 +25,38 @@
 //                                 thread and CTAs per SM at setup
 //   --theta-rows 2|4              fix the rows per dilatation thread
 //   --no-vtk                      skip the VTK files (energy/verify only)
+//   --sync-output                 write each output step's files before the
+//                                 next steps are enqueued (the reference's order)
+//   --output-threads T            threads that format VTK text (default: all)
 // Input files are read strictly: a file with fewer values than .data1
 // announces is an error (the reference reads short files silently,
 // src/helpers/utils.h:25-80).
+//
+// Output path.  At the stock cadence the reference spends as long writing
+// three ASCII VTK files per output step as it does computing (it formats them
+// serially with iostreams while the solver waits, src/main.cpp:1095-1103).
+// Here a writer thread takes each output step's state (downloaded once) from
+// a queue of at most two snapshots and writes the files while the GPU runs
+// the next steps; the text is the same (12 significant digits, %.12g, as the
+// reference's precision(12) stream), formatted in parallel with std::to_chars,
+// and the node list and vertex section that every VTK file repeats is
+// formatted once.
 #include <algorithm>
+#include <charconv>
 #include <chrono>
 #include <cmath>
+#include <condition_variable>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <deque>
 #include <fstream>
 #include <iomanip>
 #include <iostream>
+#include <mutex>
 #include <sstream>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "lps_cuda.h"
@@ -74,44 +92,166 @@ size_t count_numbers(const std::string &path) {
   return n;
 }
 
-// Legacy VTK polydata, the reference's layout (src/helpers/utils.h:95-226):
-// 12 significant digits, nodes outside the exclusion radius left out.
-void vtk_head(std::ofstream &f, const std::vector<double> &xy, const std::vector<int> &keep) {
-  f.precision(12);
-  f << "# vtk DataFile Version 3.0\n"
-    << "PD2_LPS_ABC output\n"
-    << "ASCII\n"
-    << "DATASET POLYDATA\n"
-    << "POINTS " << keep.size() << " double\n";
-  for (int i : keep) f << xy[2 * i] << " " << xy[2 * i + 1] << " 0.0\n";
-  f << "VERTICES " << keep.size() << " " << 2 * keep.size() << "\n";
-  for (size_t i = 0; i < keep.size(); i++) f << "1 " << i << "\n";
-  f << "POINT_DATA " << keep.size() << "\n";
+// ---- fast VTK text ---------------------------------------------------------
+// %.12g of v, appended to out (std::to_chars' general format with a precision
+// prints as printf does).
+inline void put_g12(std::string &out, double v) {
+  char buf[40];
+  const auto r = std::to_chars(buf, buf + sizeof buf, v, std::chars_format::general, 12);
+  out.append(buf, r.ptr);
 }
 
-bool vtk_vector(const std::string &path, const std::vector<double> &xy, const std::vector<int> &keep,
-                const std::vector<double> &v, const char *name) {
-  std::ofstream f(path);
-  if (!f) return false;
-  vtk_head(f, xy, keep);
-  f << "VECTORS " << name << " double\n";
-  for (int i : keep) f << v[2 * i] << " " << v[2 * i + 1] << " 0.0\n";
-  f << "SCALARS " << name << "_magnitude double 1\n"
-    << "LOOKUP_TABLE default\n";
-  for (int i : keep) f << std::sqrt(v[2 * i] * v[2 * i] + v[2 * i + 1] * v[2 * i + 1]) << "\n";
-  return bool(f);
+// Formats fmt(i, out) for i in [0, n) on `threads` threads in contiguous
+// ranges and returns the pieces in order.
+template <class F>
+std::vector<std::string> format_parallel(size_t n, int threads, F fmt) {
+  const int T = std::max(1, std::min<int>(threads, (int)(n / 4096) + 1));
+  std::vector<std::string> parts(T);
+  std::vector<std::thread> pool;
+  for (int t = 0; t < T; t++)
+    pool.emplace_back([&, t] {
+      const size_t a = n * t / T, b = n * (t + 1) / T;
+      std::string &o = parts[t];
+      o.reserve((b - a) * 48);
+      for (size_t i = a; i < b; i++) fmt(i, o);
+    });
+  for (auto &th : pool) th.join();
+  return parts;
 }
 
-bool vtk_scalar(const std::string &path, const std::vector<double> &xy, const std::vector<int> &keep,
-                const std::vector<double> &v, const char *name) {
-  std::ofstream f(path);
-  if (!f) return false;
-  vtk_head(f, xy, keep);
-  f << "SCALARS " << name << " double 1\n"
-    << "LOOKUP_TABLE default\n";
-  for (int i : keep) f << v[i] << "\n";
-  return bool(f);
-}
+// The three VTK files of an output step, written from a queue by one thread.
+class VtkWriter {
+ public:
+  VtkWriter(const std::vector<double> &xy, const std::vector<int> &keep, int threads)
+      : keep_(keep), threads_(threads) {
+    // header, points and vertices: the same in every file (utils.h:95-120)
+    std::string h = "# vtk DataFile Version 3.0\nPD2_LPS_ABC output\nASCII\nDATASET POLYDATA\nPOINTS " +
+                    std::to_string(keep.size()) + " double\n";
+    for (auto &p : format_parallel(keep.size(), threads, [&](size_t i, std::string &o) {
+           put_g12(o, xy[2 * keep[i]]);
+           o += ' ';
+           put_g12(o, xy[2 * keep[i] + 1]);
+           o += " 0.0\n";
+         }))
+      h += p;
+    h += "VERTICES " + std::to_string(keep.size()) + " " + std::to_string(2 * keep.size()) + "\n";
+    for (auto &p : format_parallel(keep.size(), threads, [&](size_t i, std::string &o) {
+           o += "1 ";
+           o += std::to_string(i);
+           o += '\n';
+         }))
+      h += p;
+    h += "POINT_DATA " + std::to_string(keep.size()) + "\n";
+    head_ = std::move(h);
+  }
+
+  bool vector_file(const std::string &path, const std::vector<double> &v, const char *name) const {
+    const std::string sec1 = std::string("VECTORS ") + name + " double\n";
+    const std::string sec2 = std::string("SCALARS ") + name + "_magnitude double 1\nLOOKUP_TABLE default\n";
+    auto a = format_parallel(keep_.size(), threads_, [&](size_t i, std::string &o) {
+      put_g12(o, v[2 * keep_[i]]);
+      o += ' ';
+      put_g12(o, v[2 * keep_[i] + 1]);
+      o += " 0.0\n";
+    });
+    auto b = format_parallel(keep_.size(), threads_, [&](size_t i, std::string &o) {
+      const double x = v[2 * keep_[i]], y = v[2 * keep_[i] + 1];
+      put_g12(o, std::sqrt(x * x + y * y));
+      o += '\n';
+    });
+    return write_parts(path, sec1, a, sec2, b);
+  }
+
+  bool scalar_file(const std::string &path, const std::vector<double> &v, const char *name) const {
+    const std::string sec1 = std::string("SCALARS ") + name + " double 1\nLOOKUP_TABLE default\n";
+    auto a = format_parallel(keep_.size(), threads_, [&](size_t i, std::string &o) {
+      put_g12(o, v[keep_[i]]);
+      o += '\n';
+    });
+    return write_parts(path, sec1, a, "", {});
+  }
+
+ private:
+  bool write_parts(const std::string &path, const std::string &s1, const std::vector<std::string> &a,
+                   const std::string &s2, const std::vector<std::string> &b) const {
+    FILE *f = std::fopen(path.c_str(), "wb");
+    if (!f) return false;
+    bool ok = std::fwrite(head_.data(), 1, head_.size(), f) == head_.size();
+    ok = ok && std::fwrite(s1.data(), 1, s1.size(), f) == s1.size();
+    for (const auto &p : a) ok = ok && std::fwrite(p.data(), 1, p.size(), f) == p.size();
+    ok = ok && std::fwrite(s2.data(), 1, s2.size(), f) == s2.size();
+    for (const auto &p : b) ok = ok && std::fwrite(p.data(), 1, p.size(), f) == p.size();
+    return std::fclose(f) == 0 && ok;
+  }
+
+  const std::vector<int> &keep_;
+  int threads_;
+  std::string head_;
+};
+
+// One output step's state on its way to the files.
+struct Snapshot {
+  std::string step;
+  std::vector<double> u, v, th;
+};
+
+// Writes queued snapshots in order on a thread of its own; push() blocks while
+// two snapshots are waiting, so at most three states are held on the host.
+class OutputQueue {
+ public:
+  OutputQueue(const VtkWriter &w, std::string base) : w_(w), base_(std::move(base)), th_([this] { run(); }) {}
+  ~OutputQueue() { finish(); }
+
+  void push(Snapshot &&s) {
+    std::unique_lock<std::mutex> l(mu_);
+    cv_.wait(l, [&] { return q_.size() < 2; });
+    q_.push_back(std::move(s));
+    cv_.notify_all();
+  }
+  // Waits until every queued snapshot is written; false if a write failed.
+  bool finish() {
+    {
+      std::lock_guard<std::mutex> l(mu_);
+      done_ = true;
+      cv_.notify_all();
+    }
+    if (th_.joinable()) th_.join();
+    return ok_;
+  }
+  std::string error() const { return err_; }
+
+ private:
+  void run() {
+    for (;;) {
+      Snapshot s;
+      {
+        std::unique_lock<std::mutex> l(mu_);
+        cv_.wait(l, [&] { return done_ || !q_.empty(); });
+        if (q_.empty()) return;
+        s = std::move(q_.front());
+        q_.pop_front();
+        cv_.notify_all();
+      }
+      if (!ok_) continue;
+      if (!w_.vector_file(base_ + "-" + s.step + ".vtk", s.u, "displacement") ||
+          !w_.vector_file(base_ + "-vel-" + s.step + ".vtk", s.v, "velocity") ||
+          !w_.scalar_file(base_ + "-theta-" + s.step + ".vtk", s.th, "dilatation")) {
+        ok_ = false;
+        err_ = "cannot write the VTK files of step " + s.step;
+      }
+    }
+  }
+
+  const VtkWriter &w_;
+  std::string base_;
+  std::mutex mu_;
+  std::condition_variable cv_;
+  std::deque<Snapshot> q_;
+  bool done_ = false;
+  bool ok_ = true;
+  std::string err_;
+  std::thread th_;
+};
 
 int fatal(const std::string &msg) {
   std::cerr << msg << std::endl;
@@ -130,7 +270,8 @@ int main(int argc, char **argv) {
   lps_options opt;
   lps_default_options(&opt);
   int substep = 30;
-  bool write_vtk = true;
+  bool write_vtk = true, sync_output = false;
+  int out_threads = (int)std::max(1u, std::thread::hardware_concurrency());
   for (int a = 3; a < argc; a++) {
     const std::string k = argv[a];
     auto next = [&](const char *what) -> const char * {
@@ -147,6 +288,8 @@ int main(int argc, char **argv) {
     else if (k == "--max-horizon") opt.max_horizon = std::atoi(next("--max-horizon"));
     else if (k == "--device") opt.device = std::atoi(next("--device"));
     else if (k == "--no-vtk") write_vtk = false;
+    else if (k == "--sync-output") sync_output = true;
+    else if (k == "--output-threads") out_threads = std::atoi(next("--output-threads"));
     else if (k == "--autotune") opt.autotune = 1;
     else if (k == "--theta-rows") opt.theta_rows = std::atoi(next("--theta-rows"));
     else if (k == "--precision") {
@@ -239,7 +382,9 @@ int main(int argc, char **argv) {
     keep.push_back(i);
   }
   const std::string base = job + prefix;
-  if (write_vtk && !vtk_vector(base + "-0.vtk", nodes, keep, icv, "displacement"))
+  if (out_threads <= 0) out_threads = 1;
+  VtkWriter writer(nodes, keep, out_threads);
+  if (write_vtk && !writer.vector_file(base + "-0.vtk", icv, "displacement"))
     return fatal("cannot write " + base + "-0.vtk");
   {
     std::ofstream e(base + ".energy", std::ios::out | std::ios::trunc);
@@ -251,7 +396,7 @@ int main(int argc, char **argv) {
 
   std::cout << std::endl << "Time marching started (" << n_steps << " steps):" << std::endl;
   const auto t0 = std::chrono::steady_clock::now();
-  std::vector<double> u(2 * (size_t)N), vel(2 * (size_t)N), th(N);
+  OutputQueue queue(writer, base);
   int status = 0;
   int done = 0;
   while (done < n_steps && status == 0) {
@@ -264,13 +409,23 @@ int main(int argc, char **argv) {
     const int rs = lps_read_diag(h, 0, recs.data(), (int)recs.size(), &n_rec);
     if (rs != LPS_OK && rs != LPS_ERR_NONFINITE) return fatal(lps_last_error(h));
     if (n_rec > 0 && write_vtk) {
-      if ((st = lps_download(h, 0, u.data(), vel.data(), nullptr, th.data(), nullptr)) != LPS_OK)
+      // the reference writes VTK before it checks the energy; a non-finite
+      // step ends the run below, after its log lines, as :1126-1133 do
+      Snapshot snap;
+      snap.step = std::to_string(done);
+      snap.u.resize(2 * (size_t)N);
+      snap.v.resize(2 * (size_t)N);
+      snap.th.resize(N);
+      if ((st = lps_download(h, 0, snap.u.data(), snap.v.data(), nullptr, snap.th.data(), nullptr)) != LPS_OK)
         return fatal(lps_last_error(h));
-      const std::string step_str = std::to_string(done);
-      if (!vtk_vector(base + "-" + step_str + ".vtk", nodes, keep, u, "displacement") ||
-          !vtk_vector(base + "-vel-" + step_str + ".vtk", nodes, keep, vel, "velocity") ||
-          !vtk_scalar(base + "-theta-" + step_str + ".vtk", nodes, keep, th, "dilatation"))
-        return fatal("cannot write the VTK files of step " + step_str);
+      if (sync_output) {
+        if (!writer.vector_file(base + "-" + snap.step + ".vtk", snap.u, "displacement") ||
+            !writer.vector_file(base + "-vel-" + snap.step + ".vtk", snap.v, "velocity") ||
+            !writer.scalar_file(base + "-theta-" + snap.step + ".vtk", snap.th, "dilatation"))
+          return fatal("cannot write the VTK files of step " + snap.step);
+      } else {
+        queue.push(std::move(snap));
+      }
     }
     std::ofstream e(base + ".energy", std::ios::out | std::ios::app);
     std::ofstream v(base + ".verify", std::ios::out | std::ios::app);
@@ -299,6 +454,7 @@ int main(int argc, char **argv) {
                   << "). Check dt stability." << std::endl;
     }
   }
+  if (!queue.finish()) return fatal(queue.error());
   const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   lps_destroy(h);
   if (status) return status;

@@ -13,8 +13,19 @@
    224 neighbours), nu=0.40, sigma=20 mm; 4000 steps.
 
 Geometry, absorbing ring and clouds follow the reference preprocessor
-(see ``gen``); the absorbing operators are those ``gen.disc_problem`` writes
-for the ``abc`` argument.
+(see ``gen``).  Absorbing operators: the preprocessor's least-squares fit
+(``abc="lsq"``, lps_b200.abcfit) at the time step and wavenumber range its
+stability sweep picks for that disc, read from ``SWEEP`` (the sweep itself
+costs 2-3 minutes per disc on 8 cores; ``python -m lps_b200.configs``
+recomputes the table).  Two configurations differ, for cost:
+
+* ``large``: the sweep's sample is every ring node with a truncated cloud,
+  about 12,500 at R=500 mm, so its pick is taken from the same sweep on an
+  R=20 mm disc of the same dx, m and nu; the fit itself runs on the full ring
+  (about 50,000 nodes, a minute on 16 cores);
+* ``uneven64``: fitting 64 rings (about 500,000 absorbing nodes) would take
+  about ten minutes, so this batch uses passive averaging operators
+  (``abc="average"``); kernel cost does not depend on operator values.
 """
 from __future__ import annotations
 
@@ -26,28 +37,58 @@ STEPS = {"example1": 4000, "poisson7": 4000, "large": 8000, "uneven64": 3000, "h
 POISSON_NUS = (0.15, 0.20, 0.25, 0.30, 0.35, 0.40, 0.45)
 UNEVEN_SEED = 20261203
 
+# The stability sweep's pick, (dt, delta_kappa * sqrt(c_P)), per disc
+# (R, dx, m, nu), from lps_abcfit with sweep=1 (python -m lps_b200.configs).
+SWEEP = {
+    (125.0, 0.5, 4, 0.15): (1.7e-08, 0.7),
+    (125.0, 0.5, 4, 0.20): (1.7e-08, 0.7),
+    (125.0, 0.5, 4, 0.25): (1.75e-08, 0.9),
+    (125.0, 0.5, 4, 0.30): (1.5e-08, 0.5),
+}
+# discs whose sweep is taken from a smaller disc of the same dx, m, nu
+SWEEP_PROXY = {(500.0, 0.25, 4, 0.30): (20.0, 0.25, 4, 0.30)}
+
+_cache: dict = {}
+
+
+def lsq_disc(R, dx, m, nu, n_steps, abc="lsq", **kw):
+    """gen.disc_problem with the fitted operators at the tabulated sweep pick
+    (abc="lsq"), or with the operators ``abc`` names.  Fits are cached in the
+    process (the bench builds each configuration more than once)."""
+    if abc != "lsq":
+        return gen.disc_problem(R=R, dx=dx, m=m, nu=nu, n_steps=n_steps, abc=abc, **kw)
+    key_disc = (float(R), float(dx), int(m), round(float(nu), 6))
+    pick = SWEEP.get(SWEEP_PROXY.get(key_disc, key_disc))
+    if pick is None:
+        raise KeyError(f"no sweep pick tabulated for disc {key_disc}: run python -m lps_b200.configs")
+    key = (key_disc, n_steps, tuple(sorted(kw.items())))
+    if key not in _cache:
+        _cache[key] = gen.disc_problem(R=R, dx=dx, m=m, nu=nu, n_steps=n_steps, abc="lsq", dt=pick[0],
+                                       dk_factor=pick[1], **kw)
+    return _cache[key]
+
 
 def example1(n_steps: int | None = None, nu: float = 0.25, **kw):
     n = STEPS["example1"] if n_steps is None else n_steps
-    return [gen.disc_problem(R=125.0, dx=0.5, m=4, nu=nu, n_steps=n, **kw)]
+    return [lsq_disc(125.0, 0.5, 4, nu, n, **kw)]
 
 
 def poisson7(n_steps: int | None = None, **kw):
     n = STEPS["poisson7"] if n_steps is None else n_steps
-    return [gen.disc_problem(R=125.0, dx=0.5, m=4, nu=nu, n_steps=n, **kw) for nu in POISSON_NUS]
+    return [lsq_disc(125.0, 0.5, 4, nu, n, **kw) for nu in POISSON_NUS]
 
 
 def large(n_steps: int | None = None, **kw):
     n = STEPS["large"] if n_steps is None else n_steps
-    return [gen.disc_problem(R=500.0, dx=0.25, m=4, nu=0.30, n_steps=n, sigma=40.0, centre=(50.0, -30.0), **kw)]
+    return [lsq_disc(500.0, 0.25, 4, 0.30, n, sigma=40.0, centre=(50.0, -30.0), **kw)]
 
 
 def horizon8(n_steps: int | None = None, **kw):
     n = STEPS["horizon8"] if n_steps is None else n_steps
-    return [gen.disc_problem(R=250.0, dx=0.5, m=8, nu=0.40, n_steps=n, sigma=20.0, **kw)]
+    return [lsq_disc(250.0, 0.5, 8, 0.40, n, sigma=20.0, **kw)]
 
 
-def uneven64(n_steps: int | None = None, nu_ok=None, **kw):
+def uneven64(n_steps: int | None = None, nu_ok=None, abc="average", **kw):
     """The 64 instances.  ``nu_ok(nu, m)`` may reject a draw (it is redrawn):
     the reference stops with FATAL when its lambda_PD consistency check
     (src/main.cpp:500-503, a 1e-15 relative test on rounded constants) fails,
@@ -65,7 +106,7 @@ def uneven64(n_steps: int | None = None, nu_ok=None, **kw):
         sigma = rng.uniform(0.05 * R, 0.15 * R)
         rc, ang = 0.3 * R * np.sqrt(rng.uniform()), rng.uniform(0.0, 2.0 * np.pi)
         sets.append(gen.disc_problem(R=R, dx=0.5, m=m, nu=nu, n_steps=n, amplitude=A, sigma=sigma,
-                                     centre=(rc * np.cos(ang), rc * np.sin(ang)), **kw))
+                                     centre=(rc * np.cos(ang), rc * np.sin(ang)), abc=abc, **kw))
     return sets
 
 
@@ -91,3 +132,20 @@ def build(name: str, n_steps: int | None = None, **kw):
     if name == "uneven64":
         kw.setdefault("nu_ok", nu_ok_by_create)
     return BUILDERS[name](n_steps, **kw)
+
+
+def sweep_table(discs=None):
+    """Runs the stability sweep on each disc (R, dx, m, nu) and returns
+    {disc: (dt, dk_factor)}; the default is every disc SWEEP lists plus the
+    proxies."""
+    discs = discs or sorted(set(SWEEP) | set(SWEEP_PROXY.values()))
+    out = {}
+    for R, dx, m, nu in discs:
+        s = gen.disc_problem(R=R, dx=dx, m=m, nu=nu, n_steps=1, abc="lsq")
+        out[(R, dx, m, nu)] = (s.dt, s.fit["dk_factor"])
+        print(f"    ({R}, {dx}, {m}, {nu:.2f}): ({s.dt!r}, {s.fit['dk_factor']!r}),", flush=True)
+    return out
+
+
+if __name__ == "__main__":
+    sweep_table()

@@ -13,13 +13,16 @@ file set for any R, dx, m, nu and pulse:
   (``pulse="reference"``: u_x = u_y = exp(-r^2/100) for r < 40, :1280-1289)
   or as a radial Gaussian u = A exp(-(|x-c|/sigma)^2) (x-c)/|x-c|; v = 0.
 
-Absorbing-boundary operators: the least-squares plane-wave fit of the
-reference (G_u/G_v/G_theta, :415-785) is not restated here.  ``abc="average"``
-writes operators of the same shapes and density whose rows average the
-cloud's current level (weights 1/C_i on x->x, y->y and theta^n, zero on the
-n-1 level).  They are passive (an average never grows the max-norm), so runs
-stay bounded for thousands of steps; they do not absorb like the fitted ones.
-``abc="none"`` writes no absorbing layer (constrainsNo = 0).
+Absorbing-boundary operators:
+
+* ``abc="lsq"`` -- the reference preprocessor's own: the least-squares
+  plane-wave fit of G_u, G_v and G_theta (:415-785) and, unless ``dt`` is
+  given, the (dt, delta_kappa) stability sweep that picks the time step
+  (:1047-1174), computed by ``abcfit`` (the host C++ fit in liblps_b200.so);
+* ``abc="average"`` -- passive operators of the same shapes and density whose
+  rows average the cloud's current level (weights 1/C_i on x->x, y->y and
+  theta^n, zero on the n-1 level); runs stay bounded, but nothing is absorbed;
+* ``abc="none"`` -- no absorbing layer (constrainsNo = 0).
 """
 from __future__ import annotations
 
@@ -86,14 +89,19 @@ def clouds_of(nodes: np.ndarray, centres: np.ndarray, radius: float, dx: float, 
 
 
 def disc_problem(R: float = 125.0, dx: float = 0.5, m: int = 4, nu: float = 0.25,
-                 E: float = STEEL_E, rho: float = STEEL_RHO, dt: float = 17.5e-9,
+                 E: float = STEEL_E, rho: float = STEEL_RHO, dt: float | None = None,
                  n_steps: int = 4000, pulse="baseline", amplitude: float = 1e-3,
                  sigma: float | None = None, centre=(0.0, 0.0), abc: str = "average",
-                 abcs_step: int = 2, jitter: float = 0.0, seed: int = 0) -> InputSet:
-    """Build one input set (see the module docstring).  ``jitter`` > 0 moves
-    every node by a seeded uniform offset of up to jitter*dx per coordinate,
-    so the node set is no longer a lattice (horizons then come from the
-    distance search alone, as for an arbitrary node file)."""
+                 abcs_step: int = 2, jitter: float = 0.0, seed: int = 0, dk_factor: float = 1.0,
+                 fit_threads: int = 0) -> InputSet:
+    """Build one input set (see the module docstring).  ``dt``: the time step;
+    None means 17.5 ns (the reference preprocessor's pick at nu=0.25) for
+    ``abc`` "average" and "none", and the stability sweep's pick for "lsq"
+    (given a dt, "lsq" fits at that dt and delta_kappa = dk_factor /
+    sqrt(c_P)).  ``jitter`` > 0 moves every node by a seeded uniform offset of
+    up to jitter*dx per coordinate, so the node set is no longer a lattice
+    (horizons then come from the distance search alone, as for an arbitrary
+    node file)."""
     dy = dx
     delta = m * dx
     nodes = disc_lattice(R, dx, dy)
@@ -121,16 +129,32 @@ def disc_problem(R: float = 125.0, dx: float = 0.5, m: int = 4, nu: float = 0.25
         raise ValueError(f"unknown pulse {pulse!r}")
     v0 = np.zeros(2 * N)
     bct = -np.ones(2 * N, np.int32)
+    if dt is None and abc != "lsq":
+        dt = 17.5e-9
     s = InputSet(n_nodes=N, n_steps=n_steps, n_abc=0, max_cloud=0, E=E, nu=nu, rho=rho, dt=dt,
                  delta=delta, dx=dx, dy=dy, nodes=nodes, bctypes=bct, u0=u0, v0=v0,
-                 t1=n_steps * dt, s0=math.sqrt(5.0 * math.pi * STEEL_G0 / (12.0 * E * delta)))
+                 t1=n_steps * (dt or 0.0), s0=math.sqrt(5.0 * math.pi * STEEL_G0 / (12.0 * E * delta)))
     if abc == "none":
         return s
-    if abc != "average":
+    if abc not in ("average", "lsq"):
         raise ValueError(f"unknown abc {abc!r}")
     ring = np.nonzero(r > R - delta)[0].astype(np.int32)
     clouds, C = clouds_of(nodes, ring, delta, dx, dy)
     NA = ring.size
+    bct[2 * ring] = 1
+    bct[2 * ring + 1] = 1
+    s.n_abc, s.max_cloud = NA, C
+    s.inf_nodes, s.clouds = ring, clouds
+    s.bctypes = bct
+    if abc == "lsq":
+        from . import abcfit
+        f = abcfit.fit(nodes, ring, clouds, E=E, nu=nu, rho=rho, delta=delta, dx=dx, dy=dy, abcs_step=abcs_step,
+                       sweep=dt is None, dt=dt, dk_factor=dk_factor, n_threads=fit_threads)
+        s.dt = f["dt"]
+        s.t1 = n_steps * s.dt
+        s.gu, s.gv, s.gtheta = f["gu"], f["gv"], f["gtheta"]
+        s.fit = {k: v for k, v in f.items() if k not in ("gu", "gv", "gtheta")}
+        return s
     cnt = (clouds >= 0).sum(axis=1).astype(np.float64)
     w = np.where(clouds >= 0, 1.0 / cnt[:, None], 0.0)
     cpc = 2 * abs(abcs_step)
@@ -139,12 +163,7 @@ def disc_problem(R: float = 125.0, dx: float = 0.5, m: int = 4, nu: float = 0.25
     gu[1::2, 1::cpc] = w      # y^{n} -> y
     gth = np.zeros((NA, abs(abcs_step) * C))
     gth[:, 0::abs(abcs_step)] = w
-    bct[2 * ring] = 1
-    bct[2 * ring + 1] = 1
-    s.n_abc, s.max_cloud = NA, C
-    s.inf_nodes, s.clouds = ring, clouds
     s.gu, s.gv, s.gtheta = gu, gu.copy(), gth
-    s.bctypes = bct
     return s
 
 

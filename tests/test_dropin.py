@@ -128,3 +128,22 @@ def test_nonfinite_state_is_fatal(tmp_path):
     assert "FATAL: Energy is NaN/Inf at step 30!" in r.stderr
     # the record of the failing step is written before the exit, as the reference does
     assert len(open(tmp_path / "r10_nan.energy").read().splitlines()) == 2
+
+
+@pytest.mark.gpu
+def test_async_and_sync_output_write_the_same_bytes(tmp_path):
+    """The background VTK writer (default) and --sync-output (each output
+    step's files written before the next steps) produce identical files."""
+    s = load_inputs("r10")
+    for mode in ("async", "sync"):
+        d = tmp_path / mode
+        d.mkdir()
+        write_input_set(str(d / "r10"), s)
+        extra = ["--sync-output"] if mode == "sync" else ["--output-threads", "3"]
+        r = run_exe(d, "_o", "r10", *extra)
+        assert r.returncode == 0, r.stderr
+    names = sorted(f for f in os.listdir(tmp_path / "async") if f.startswith("r10_o"))
+    assert len(names) == 2 + 1 + 3 * (s.n_steps // 30)
+    assert names == sorted(f for f in os.listdir(tmp_path / "sync") if f.startswith("r10_o"))
+    for f in names:
+        assert open(tmp_path / "async" / f, "rb").read() == open(tmp_path / "sync" / f, "rb").read(), f

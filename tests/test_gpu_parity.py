@@ -180,3 +180,26 @@ def test_autotune_changes_no_result(precision):
             for key in ("u", "v", "a", "theta"):
                 np.testing.assert_array_equal(out[other][k][1][key], out[False][k][1][key])
             np.testing.assert_array_equal(out[other][k][0]["E"], out[False][k][0]["E"])
+
+
+@pytest.mark.parametrize("kind", ["lattice_m8", "jittered_m4"])
+def test_gpu_horizon_search_equals_host(kind):
+    """The horizon search on the GPU (lps_horizons.cu) gives the host bucket
+    grid's horizons: same weighted volumes bit for bit and the same state,
+    bit for bit, after some steps on the neighbour-list kernels."""
+    if kind == "lattice_m8":
+        s = gen.disc_problem(R=30.0, dx=0.5, m=8, nu=0.3, n_steps=40, sigma=5.0)
+        opts = dict(max_horizon=256)
+    else:
+        s = gen.disc_problem(R=30.0, dx=0.5, m=4, nu=0.3, n_steps=40, sigma=5.0, jitter=0.2, seed=11)
+        opts = {}
+    out = {}
+    for build in ("host", "gpu"):
+        with Solver(s, path="csr", horizon_build=build, **opts) as sv:
+            info = sv.info(0)
+            assert info["horizon_on_gpu"] == (build == "gpu")
+            sv.step(40, diag_every=20)
+            out[build] = (sv.download(0), info["max_horizon_len"])
+    assert out["host"][1] == out["gpu"][1]
+    for key in ("m", "u", "v", "a", "theta"):
+        np.testing.assert_array_equal(out["host"][0][key], out["gpu"][0][key])
