@@ -4,13 +4,15 @@
 Workload (default ``poisson7``): the Poisson-ratio batch -- seven instances of
 the Example 1 geometry (R=125 mm, dx=0.5 mm, m=4: 196,321 nodes, 6,268
 absorbing nodes, cloud size 49 each) with nu in {0.15,...,0.45}, a radial
-Gaussian pulse (A=1e-3 mm, sigma=40/3 mm), dt=17.5 ns, run together in one
-handle for 4000 time steps with diagnostics every 30 steps (the reference's
-output cadence, src/main.cpp:34,981).  One bench step = one complete run of
-the batch from its initial state.  Inputs are synthetic (lps_b200.gen):
-geometry, rings and clouds equal the reference preprocessor's; the absorbing
-operators are passive averaging operators of the same shape (the reference's
-least-squares fit is not restated).
+Gaussian pulse (A=1e-3 mm, sigma=40/3 mm), run together in one handle for
+4000 time steps with diagnostics every 30 steps (the reference's output
+cadence, src/main.cpp:34,981).  One bench step = one complete run of the batch
+from its initial state.  Inputs are synthetic (lps_b200.gen, lps_b200.configs):
+geometry, rings and clouds equal the reference preprocessor's, and each
+instance carries its own least-squares absorbing operators, time step and
+wavenumber range from the preprocessor's stability sweep (lps_b200.abcfit);
+the 64-instance batch alone uses passive averaging operators of the same
+shape.
 
 ``--impl reference`` times the reference solver itself (compiled from its
 sources into oracle/_ref/, output off) on the host cores instead.
@@ -77,6 +79,11 @@ WORKLOAD_TEXT = {
     "horizon8": "large-horizon disc (R=250 mm, dx=0.5 mm, m=8: 224 neighbours, nu=0.40)",
 }
 NEIGHBOURS = {3: 36, 4: 68, 5: 96, 8: 224}
+_LSQ = ("synthetic, seeded (generated geometry, ring and clouds as the reference preprocessor builds them; "
+        "least-squares absorbing operators, dt and delta_kappa from its stability sweep, per instance)")
+DATA_TEXT = {"poisson7": _LSQ, "example1": _LSQ, "large": _LSQ, "horizon8": _LSQ,
+             "uneven64": "synthetic, seeded (generated geometry, ring and clouds; passive averaging absorbing "
+                         "operators of the same shape, dt = 17.5 ns)"}
 
 
 def workload_sets(name, n_steps):
@@ -376,7 +383,7 @@ def run_ours(args, rank, world, local_rank, precision, with_cpu=True):
     out = {"metric": METRIC, "value": value, "unit": "node-steps/s", "n_gpus": world, "steps": K,
            "warmup": W, "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64" if precision == "fp64" else "f32+f64",
-           "data": "synthetic (generated Example-1 geometry; passive averaging ABC operators)",
+           "data": DATA_TEXT[args.workload],
            "config": workload_config(args.workload, sets, args) | {"parallelism": f"replicas{world}"},
            "e2e": {"value": e2e_value, "unit": "node-steps/s", "h2d_bytes_per_step": h2d,
                    "d2h_bytes_per_step": d2h,
@@ -407,7 +414,7 @@ def run_reference(args):
     return {"metric": METRIC, "value": v, "unit": "node-steps/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * sec / (args.warmup + args.steps),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (generated Example-1 geometry; passive averaging ABC operators)",
+            "data": DATA_TEXT[args.workload],
             "config": workload_config(args.workload, sets, args) | {"parallelism": "openmp"},
             "impl": "reference",
             "cpu_baseline": {"value": v, "unit": "node-steps/s", "cores": threads, "kind": kind,

@@ -422,22 +422,35 @@ template <int M>
 static void static32_m(const std::vector<uint8_t> &type, int pitch, long first, long count, std::vector<float2> &w32,
                        std::vector<float4> &ka32) {
   constexpr Sten<M> sten = make_sten<M>();
+  constexpr int N = Sten<M>::N;
+  // per-offset terms, evaluated once (sten_qd's square root is an iteration
+  // meant for compile-time tables)
+  double tw[N][2], tk[N][3];
+  long nb_off[N];
+  for (int j = 0; j < N; j++) {
+    const int a = sten.a[j], b = sten.b[j];
+    tw[j][0] = sten_qd(kWx, M, a, b);
+    tw[j][1] = sten_qd(kWy, M, a, b);
+    // beta xi_hat xi_hat^T = g xi_hat^T with g = beta xi_hat
+    const double gx = sten_qd(kGx, M, a, b), gy = sten_qd(kGy, M, a, b);
+    const double hx = sten_qd(kHx, M, a, b), hy = sten_qd(kHy, M, a, b);
+    tk[j][0] = gx * hx;
+    tk[j][1] = gx * hy;
+    tk[j][2] = gy * hy;
+    nb_off[j] = (long)a * pitch + b;
+  }
+#pragma omp parallel for schedule(static)
   for (long c = first; c < first + count; c++) {
     if (!(type[c] & kExists)) continue;
     double wx = 0, wy = 0, kxx = 0, kxy = 0, kyy = 0;
-    for (int j = 0; j < Sten<M>::N; j++) {
-      const int a = sten.a[j], b = sten.b[j];
-      const long nb = c + (long)a * pitch + b;
-      if (type[nb] & kExists) {
-        wx += sten_qd(kWx, M, a, b);
-        wy += sten_qd(kWy, M, a, b);
+    for (int j = 0; j < N; j++) {
+      if (type[c + nb_off[j]] & kExists) {
+        wx += tw[j][0];
+        wy += tw[j][1];
       } else {
-        // beta xi_hat xi_hat^T = g xi_hat^T with g = beta xi_hat
-        const double gx = sten_qd(kGx, M, a, b), gy = sten_qd(kGy, M, a, b);
-        const double hx = sten_qd(kHx, M, a, b), hy = sten_qd(kHy, M, a, b);
-        kxx += gx * hx;
-        kxy += gx * hy;
-        kyy += gy * hy;
+        kxx += tk[j][0];
+        kxy += tk[j][1];
+        kyy += tk[j][2];
       }
     }
     w32[c] = make_float2((float)wx, (float)wy);

@@ -44,6 +44,11 @@ SWEEP = {
     (125.0, 0.5, 4, 0.20): (1.7e-08, 0.7),
     (125.0, 0.5, 4, 0.25): (1.75e-08, 0.9),
     (125.0, 0.5, 4, 0.30): (1.5e-08, 0.5),
+    (125.0, 0.5, 4, 0.35): (1.75e-08, 0.8999999999999999),
+    (125.0, 0.5, 4, 0.40): (1.7e-08, 0.7),
+    (125.0, 0.5, 4, 0.45): (1.6e-08, 0.7),
+    (20.0, 0.25, 4, 0.30): (8e-09, 0.7),
+    (250.0, 0.5, 8, 0.40): (5e-09, 2.0),
 }
 # discs whose sweep is taken from a smaller disc of the same dx, m, nu
 SWEEP_PROXY = {(500.0, 0.25, 4, 0.30): (20.0, 0.25, 4, 0.30)}
