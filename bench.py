@@ -241,13 +241,15 @@ def algorithmic_bytes(sets, kernel, precision="fp64"):
     f32 = precision == "fp32_mixed"
     step_node = 140 if f32 else 168
     table = {
-        # FP64: read u_pred 16, theta 8, coef 16, vh 16; write a 16, v 16,
-        # vh 16, u_pred(next) 16.  FP32-mixed: read u_pred32 8, theta 8,
-        # coef32 8, vh 16, u_pred 16; write a 16, v 16, vh 16, u_pred(next) 16,
-        # u_pred32(next) 8
-        "force_tiles": ((128 if f32 else 120) * n, (56 if f32 else 80) * n),
-        # dilatation: read u_pred 16 (FP32-mixed: 8), m 8; write theta 8
-        "theta_tiles": ((24 if f32 else 32) * n, None),
+        # an ordinary (not full) step at an interior node -- v, a and theta are
+        # written only where later steps read them, and on full steps:
+        # FP64: read u_pred 16, theta 8, coef 16, vh 16; write vh 16,
+        # u_pred(next) 16.  FP32-mixed: read u_pred32 8, A' 4, vh 16, u_pred 16;
+        # write vh 16, u_pred(next) 16, u_pred32(next) 8
+        "force_tiles": ((84 if f32 else 88) * n, (56 if f32 else 80) * n),
+        # dilatation: FP64 read u_pred 16, m 8, write theta 8; FP32-mixed read
+        # u_pred32 8, write A' 4 (full tiles need no m and no B')
+        "theta_tiles": ((12 if f32 else 32) * n, None),
         # G_u, G_v of the step and G_theta of the next: 18C doubles + 4C index
         # bytes per ABC node (the gathered state hits L2)
         "abc_sell": (148 * abc, 148 * abc),
@@ -263,12 +265,13 @@ def algorithmic_bytes(sets, kernel, precision="fp64"):
     return table.get(kernel, (None, None))
 
 
-def measured_traffic(kernel, precision):
-    """DRAM bytes per launch from the committed ncu summaries, if listed."""
+def measured_traffic(kernel, precision, workload):
+    """DRAM bytes per launch of `kernel` on `workload` from the committed ncu
+    summaries (profiles/ncu_traffic.json), if listed."""
     p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if not os.path.exists(p):
         return None
-    d = json.load(open(p))
+    d = json.load(open(p)).get(workload, {})
     return d.get(precision, {}).get(kernel, {}).get("dram_bytes_per_launch")
 
 
@@ -284,8 +287,9 @@ def run_ours(args, rank, world, local_rank, precision, with_cpu=True):
     dev = torch.device("cuda", local_rank)
     sets = workload_sets(args.workload, args.time_steps)
     stream = torch.cuda.Stream(device=dev)
+    wide = max(int(round(s.delta / s.dx)) for s in sets) > 5  # m = 8: 225 horizon entries
     sv = Solver(sets, precision=precision, path=args.path, device=local_rank,
-                stream=stream.cuda_stream, autotune=not args.no_autotune)
+                stream=stream.cuda_stream, autotune=not args.no_autotune, max_horizon=256 if wide else 128)
     info = sv.info(0)
     T, K, W = args.time_steps, args.steps, args.warmup
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
@@ -369,11 +373,13 @@ def run_ours(args, rank, world, local_rank, precision, with_cpu=True):
     for k, v in prof.items():
         b, _ = algorithmic_bytes(sets, k, precision)
         kernels[k] = {"launches": v[0], "ms_per_launch": v[1] / v[0], "algorithmic_bytes": b,
-                      "achieved_gbs": gbs(b, v[1] / v[0]), "traffic": measured_traffic(k, precision)}
+                      "achieved_gbs": gbs(b, v[1] / v[0]),
+                      "traffic": measured_traffic(k, precision, args.workload)}
     step_bytes, _ = algorithmic_bytes(sets, "step", precision)
     roofline = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
-                "traffic": measured_traffic(name, precision), "algorithmic_bytes_per_launch": ab_grade or ab,
+                "traffic": measured_traffic(name, precision, args.workload),
+                "algorithmic_bytes_per_launch": ab_grade or ab,
                 "actual_layout_bytes_per_launch": ab, "ms_per_launch": per_launch_ms,
                 "kernels": kernels, "serialized_step_ms": step_ms,
                 "step_algorithmic_bytes": step_bytes,
@@ -391,7 +397,7 @@ def run_ours(args, rank, world, local_rank, precision, with_cpu=True):
                                "absorbing-boundary operators), as the reference's timer excludes its setup"},
            "gpu_launches": launches, "roofline": roofline, "clocks": clk,
            "kernel_path": info["path"], "tile_ctas": [info["tile_ctas_theta"], info["tile_ctas_force"]],
-           "tile_rows_theta": info["tile_rows_theta"],
+           "tile_rows_theta": info["tile_rows_theta"], "tile_rows_force": info["tile_rows_force"],
            "final_dE_rel": final_dE, "_u": final_u}
     if with_cpu and rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1

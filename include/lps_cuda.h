@@ -99,7 +99,9 @@ typedef struct lps_options {
   int32_t horizon_build;    /* horizon search (src/main.cpp:352-356): 0 auto  */
                             /* (on the GPU from 50,000 nodes), 1 host bucket  */
                             /* grid, 2 GPU; both give the same horizons       */
-  int32_t pad;
+  int32_t force_rows;       /* dense FP32-mixed force rows per thread: 0      */
+                            /* (default: 2, or the autotuner's choice), 2 or  */
+                            /* 4 (fixed); the FP64 force pass always has 2    */
 } lps_options;
 
 /* One output record: the .energy columns (src/main.cpp:1108-1112), the
@@ -121,8 +123,8 @@ typedef struct lps_info {
   int32_t n_abc_m_corrected, pad;                             /* instance 0   */
   int32_t tile_ctas_theta, tile_ctas_force;  /* dense path: CTAs per SM of the */
                                              /* dilatation / force tiles      */
-  int32_t tile_rows_theta, pad2;             /* dense path: rows per thread of */
-                                             /* the dilatation tiles          */
+  int32_t tile_rows_theta, tile_rows_force;  /* dense path: rows per thread of */
+                                             /* the dilatation / force tiles  */
   double horizon_ms;                         /* instance: horizon search time */
   int32_t horizon_on_gpu, pad3;              /* 1: searched on the GPU        */
 } lps_info;

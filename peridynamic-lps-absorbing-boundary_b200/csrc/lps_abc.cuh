@@ -36,6 +36,13 @@ __device__ __forceinline__ void write_ab32(float2 *ab32, const float2 *coef32, i
                           : make_float2(0.f, P.dense ? 0.f : -1.f);
 }
 
+// The dense path's FP32-mixed form keeps A' and B' as separate planes; B' is
+// static, so only A' (with its factor dx) is written wherever theta is.
+__device__ __forceinline__ void write_ap32(float *ap32, const float *bp32, int node, double th, const InstParams &P) {
+  const float q = bp32[node];
+  ap32[node] = q > 0.f ? (float)(th * P.f32_ab) * q * (float)P.dx : 0.f;
+}
+
 // G_theta at one ABC node per warp, src/main.cpp:795-812 (and, in the
 // FP32-mixed form, the node's force coefficients).
 __device__ __forceinline__ void abc_theta_warp(const Abc &ab, int a, const double *__restrict__ th_n,

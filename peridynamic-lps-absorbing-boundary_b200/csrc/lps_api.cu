@@ -65,6 +65,8 @@ struct lps_handle {
   float2 *U32[2] = {};        // FP32-mixed form: FP32 copies of the predicted level, by step parity
   float2 *coef32 = nullptr;   // FP32-mixed form: (q, q) with q = m_ref / m_i; (0, -1) where m_i <= 0
   float2 *AB32 = nullptr;     // FP32-mixed CSR form: force coefficients (A', B'), written with theta
+  float *AP32 = nullptr;      // FP32-mixed dense form: force coefficient plane A', written with theta
+  float *BP32 = nullptr;      // FP32-mixed dense form: static force coefficient plane B' = q
   // diagnostics
   DiagPartial *partials = nullptr;
   DiagRecord *log = nullptr;
@@ -172,6 +174,8 @@ void pack_abc(const lps_problem &p, const lps_options &o, const InstanceSetup &s
     // pads odd clouds) so that every operator row starts 16-byte aligned
     const int len = (int)js.size() + ((int)js.size() & 1);
     for (int j : js) H.cl_idx.push_back(gmap(p.clouds[(size_t)i * C + j]));
+    if (writes)
+      for (int j : js) type[gmap(p.clouds[(size_t)i * C + j])] |= kKeepState;
     if (len > (int)js.size()) H.cl_idx.push_back(gmap(node));
     const double *g0 = p.gu + (size_t)(2 * i) * cols, *g1 = p.gu + (size_t)(2 * i + 1) * cols;
     const double *h0 = p.gv + (size_t)(2 * i) * cols, *h1 = p.gv + (size_t)(2 * i + 1) * cols;
@@ -207,6 +211,7 @@ void pack_abc(const lps_problem &p, const lps_options &o, const InstanceSetup &s
         const double ry = p.nodes[2 * nb + 1] - p.nodes[2 * node + 1];
         const double dist = std::sqrt(rx * rx + ry * ry);
         H.idw_idx.push_back(gmap(nb));
+        type[gmap(nb)] |= kKeepState;
         H.idw_w.push_back(1.0 / (dist + 1e-30));
         il++;
       }
@@ -238,6 +243,7 @@ void fill_params(InstParams &P, const lps_problem &p, const lps_options &o, cons
   P.out_r = s.out_r;
   P.f32_b0 = s.alpha;
   P.f32_ab = (s.lam - s.mu) / (4.0 * s.mu);
+  P.mref = s.m_ref;
   P.kinematic = o.kinematic_v;
   P.theta_method = o.theta_method;
   P.abcs_step = o.abcs_step;
@@ -675,12 +681,15 @@ int build_dense(lps_handle *h, const lps_problem *probs, const std::vector<Latti
     std::vector<float4> ka32(n, make_float4(0.f, 0.f, 0.f, 0.f));
     for (int k = 0; k < K; k++)
       dense32_static(lat[k].M, type, P, D.host_cell_begin[k], D.host_cells[k], w32, ka32);
+    // B' = q where the cell exists with m_i > 0, else 0
+    std::vector<float> bp32(n, 0.f);
+    for (int c = 0; c < n; c++) bp32[c] = coef32[c].y > 0.f ? coef32[c].y : 0.f;
     float2 *d_w32;
     float4 *d_ka32;
-    if ((st = dev_upload(h, &h->coef32, coef32)) || (st = dev_upload(h, &d_w32, w32)) ||
+    if ((st = dev_upload(h, &h->BP32, bp32)) || (st = dev_upload(h, &d_w32, w32)) ||
         (st = dev_upload(h, &d_ka32, ka32)))
       return st;
-    D.d32.coef32 = h->coef32;
+    D.d32.bp32 = h->BP32;
     D.d32.w32 = d_w32;
     D.d32.ka32 = d_ka32;
   }
@@ -709,7 +718,7 @@ int finish_dense(lps_handle *h) {
   const uint8_t *type = h->lg.geo.type;
   for (auto &gr : D.groups) {
     const int s = dense_encode_maps(gr, D.pitch, D.total_rows, h->U, h->TH, coef, type, D.fp32 ? h->U32 : nullptr,
-                                    h->AB32, h->err);
+                                    h->AP32, h->BP32, h->err);
     if (s) return s;
   }
   LPS_CUDA_TRY(h, cudaStreamCreateWithFlags(&D.side, cudaStreamNonBlocking));
@@ -743,7 +752,7 @@ StepPtrs step_ptrs(lps_handle *h, int64_t n) {
   p.u_np1 = h->U[(n + 1) % R];
   p.u_np2 = h->U[(n + 2) % R];
   p.th_ring = u1;
-  p.pad = 0;
+  p.full = 1;
   p.v_n = h->V[u0];
   p.v_nm1 = h->V[um];
   p.v_np1 = h->V[u1];
@@ -761,8 +770,9 @@ StepPtrs step_ptrs(lps_handle *h, int64_t n) {
 
 // Kernels of one step (and its diagnostics); returns the launch count.
 // `mark`, when set, is called after each launch with the kernel's name.
-int enqueue_step(lps_handle *h, int64_t n, bool diag, const Mark *mark = nullptr) {
-  const StepPtrs p = step_ptrs(h, n);
+int enqueue_step(lps_handle *h, int64_t n, bool diag, bool full, const Mark *mark = nullptr) {
+  StepPtrs p = step_ptrs(h, n);
+  p.full = (diag || full) ? 1 : 0;
   cudaStream_t st = h->stream;
   auto M = [&](const char *name) {
     if (mark) (*mark)(name);
@@ -830,12 +840,13 @@ int get_graph(lps_handle *h, int mask, cudaGraphExec_t *out);
 // it is at least 2 % faster.  None of these changes a result: tiles come from
 // a counter and each cell's arithmetic is the same whichever CTA and thread
 // computes it.  The caller resets the state afterwards.
-int autotune_dense(lps_handle *h, int rows_only) {
-  int max_f = 1, max_t[2] = {1, 1};  // [0]: four rows, [1]: two rows
+int autotune_dense(lps_handle *h, int rows_only, int force_rows_only) {
+  int max_f[2] = {1, 0}, max_t[2] = {1, 1};  // [0]: two-row force / four-row dilatation, [1]: the other form
   for (const auto &gr : h->dg.groups) {
     max_t[0] = std::max(max_t[0], gr.max_theta_ctas);
     max_t[1] = std::max(max_t[1], gr.max_theta_ctas2);
-    max_f = std::max(max_f, gr.max_force_ctas);
+    max_f[0] = std::max(max_f[0], gr.max_force_ctas);
+    max_f[1] = std::max(max_f[1], gr.max_force_ctas4);
   }
   // the two timing events, destroyed on every return path
   struct EventPair {
@@ -853,8 +864,8 @@ int autotune_dense(lps_handle *h, int rows_only) {
     h->graphs.clear();
     h->graph_kernels.clear();
   };
-  auto time_choice = [&](int rows, int t, int f, float *ms_out) -> int {
-    dense_set_ctas(h->dg, rows, t, f);
+  auto time_choice = [&](int rows, int t, int fr, int f, float *ms_out) -> int {
+    dense_set_ctas(h->dg, rows, t, f, fr);
     drop_graphs();
     cudaGraphExec_t ex;
     int st = get_graph(h, 0, &ex);
@@ -876,30 +887,36 @@ int autotune_dense(lps_handle *h, int rows_only) {
     return LPS_OK;
   };
   const int rows0 = rows_only == 2 ? 2 : 4, r0 = rows0 == 4 ? 0 : 1;
+  const int fr0 = force_rows_only == 4 && max_f[1] > 0 ? 4 : 2, f0 = fr0 == 2 ? 0 : 1;
   float ref = 0.f;
-  int st = time_choice(rows0, max_t[r0], max_f, &ref);
+  int st = time_choice(rows0, max_t[r0], fr0, max_f[f0], &ref);
   float best = ref;
-  int best_r = rows0, best_t = max_t[r0], best_f = max_f;
+  int best_r = rows0, best_t = max_t[r0], best_fr = fr0, best_f = max_f[f0];
   for (int rows : {4, 2}) {
     if (rows_only && rows != rows_only) continue;
     const int mt = max_t[rows == 4 ? 0 : 1];
-    for (int t = 1; t <= mt && st == LPS_OK; t++)
-      for (int f = 1; f <= max_f && st == LPS_OK; f++) {
-        if (rows == rows0 && t == mt && f == max_f) continue;
-        float ms = 0.f;
-        if ((st = time_choice(rows, t, f, &ms))) break;
-        if (ms < best && ms < 0.98f * ref) {
-          best = ms;
-          best_r = rows;
-          best_t = t;
-          best_f = f;
+    for (int fr : {2, 4}) {
+      if ((force_rows_only && fr != force_rows_only) || max_f[fr == 2 ? 0 : 1] == 0) continue;
+      const int mf = max_f[fr == 2 ? 0 : 1];
+      for (int t = 1; t <= mt && st == LPS_OK; t++)
+        for (int f = 1; f <= mf && st == LPS_OK; f++) {
+          if (rows == rows0 && t == mt && fr == fr0 && f == mf) continue;
+          float ms = 0.f;
+          if ((st = time_choice(rows, t, fr, f, &ms))) break;
+          if (ms < best && ms < 0.98f * ref) {
+            best = ms;
+            best_r = rows;
+            best_t = t;
+            best_fr = fr;
+            best_f = f;
+          }
         }
-      }
+    }
   }
   drop_graphs();
   if (st == LPS_OK) st = check_device_error(h);
   if (st) return st;
-  dense_set_ctas(h->dg, best_r, best_t, best_f);
+  dense_set_ctas(h->dg, best_r, best_t, best_f, best_fr);
   return LPS_OK;
 }
 
@@ -924,6 +941,7 @@ int drain_log(lps_handle *h) {
 // a graph that starts on a multiple of it finds every buffer where it
 // captured it.
 int graph_period(const lps_handle *h) { return h->ring_u == 4 ? 12 : 6; }
+constexpr int kFullBit = 16;  // graph masks: bits 0..11 diagnostics, 16..27 full steps
 
 int check_device_error(lps_handle *h) {
   if (h->path != LPS_PATH_DENSE || !h->dg.d_err) return LPS_OK;
@@ -945,7 +963,10 @@ int get_graph(lps_handle *h, int mask, cudaGraphExec_t *out) {
   cudaGraph_t g;
   LPS_CUDA_TRY(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
   int kernels = 0;
-  for (int r = 0; r < graph_period(h); r++) kernels += enqueue_step(h, r, (mask >> r) & 1);
+  // mask bit r: diagnostics after step r; bit kFullBit + r: step r is full
+  // (StepPtrs::full) without diagnostics
+  for (int r = 0; r < graph_period(h); r++)
+    kernels += enqueue_step(h, r, (mask >> r) & 1, (mask >> (kFullBit + r)) & 1);
   LPS_CUDA_TRY(h, cudaStreamEndCapture(h->stream, &g));
   cudaGraphExec_t ex;
   cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
@@ -1043,10 +1064,16 @@ int alloc_state(lps_handle *h) {
       if ((s = dev_alloc(h, &h->U32[r], n))) return s;
       LPS_CUDA_TRY(h, cudaMemset(h->U32[r], 0, sizeof(float2) * n));
     }
-    // force coefficients, zero at absent cells (the dense kernels rely on it)
-    if ((s = dev_alloc(h, &h->AB32, n))) return s;
-    LPS_CUDA_TRY(h, cudaMemset(h->AB32, 0, sizeof(float2) * n));
-    h->dg.d32.ab32 = h->AB32;
+    // force coefficients, zero at absent cells (the dense kernels rely on it):
+    // (A', B') pairs on the neighbour-list path, the A' plane on the dense path
+    if (h->path == LPS_PATH_DENSE) {
+      if ((s = dev_alloc(h, &h->AP32, n))) return s;
+      LPS_CUDA_TRY(h, cudaMemset(h->AP32, 0, sizeof(float) * n));
+      h->dg.d32.ap32 = h->AP32;
+    } else {
+      if ((s = dev_alloc(h, &h->AB32, n))) return s;
+      LPS_CUDA_TRY(h, cudaMemset(h->AB32, 0, sizeof(float2) * n));
+    }
   }
   // diagnostics partials: node blocks (CSR) or tiles (dense), then ABC blocks
   int n_tiles = 0;
@@ -1134,6 +1161,10 @@ int lps_create(const lps_problem *problems, int n_instances, const lps_options *
   }
   if (o.theta_rows != 0 && o.theta_rows != 2 && o.theta_rows != 4) {
     g_create_error = "lps_create: theta_rows must be 0, 2 or 4";
+    return LPS_ERR_INVALID_ARG;
+  }
+  if (o.force_rows != 0 && o.force_rows != 2 && o.force_rows != 4) {
+    g_create_error = "lps_create: force_rows must be 0, 2 or 4";
     return LPS_ERR_INVALID_ARG;
   }
   if (o.precision != LPS_FP64 && o.precision != LPS_FP32_MIXED) {
@@ -1238,8 +1269,10 @@ int lps_create(const lps_problem *problems, int n_instances, const lps_options *
     }
   }
   if ((s = do_reset(h))) return fail(s);
-  if (h->path == LPS_PATH_DENSE && o.theta_rows == 2) dense_set_ctas(h->dg, 2, 1 << 20, 1 << 20);
-  if (o.autotune && h->path == LPS_PATH_DENSE && (s = autotune_dense(h, o.theta_rows))) return fail(s);
+  if (h->path == LPS_PATH_DENSE && (o.theta_rows == 2 || o.force_rows == 4))
+    dense_set_ctas(h->dg, o.theta_rows == 2 ? 2 : 4, 1 << 20, 1 << 20, o.force_rows == 4 ? 4 : 2);
+  if (o.autotune && h->path == LPS_PATH_DENSE && (s = autotune_dense(h, o.theta_rows, o.force_rows)))
+    return fail(s);
   if (o.autotune && h->path == LPS_PATH_DENSE && (s = do_reset(h))) return fail(s);
   if (cudaStreamSynchronize(h->stream) != cudaSuccess) {
     h->err = std::string("setup kernels failed: ") + cudaGetErrorString(cudaGetLastError());
@@ -1293,6 +1326,8 @@ int lps_step(lps_handle *h, int n_steps, int diag_every) {
       if (diag_every > 0 && s % diag_every == 0) {
         mask |= 1 << r;
         new_rec++;
+      } else if (remaining - r == 1) {
+        mask |= 1 << (kFullBit + r);  // the call's last step leaves every field current
       }
     }
     if (h->pending_records + new_rec > h->log_capacity) {
@@ -1306,7 +1341,7 @@ int lps_step(lps_handle *h, int n_steps, int diag_every) {
       LPS_CUDA_TRY(h, cudaGraphLaunch(ex, h->stream));
       h->launches += h->graph_kernels[mask];
     } else {
-      h->launches += enqueue_step(h, h->step, mask & 1);
+      h->launches += enqueue_step(h, h->step, mask & 1, (mask >> kFullBit) & 1);
       LPS_CUDA_TRY(h, cudaGetLastError());
     }
     h->step += chunk;
@@ -1435,6 +1470,7 @@ int lps_get_info(lps_handle *h, int instance, lps_info *info) {
     info->tile_ctas_theta = (g0.grid_theta + n_sm - 1) / n_sm;
     info->tile_ctas_force = (g0.grid_force + n_sm - 1) / n_sm;
     info->tile_rows_theta = g0.theta_rows;
+    info->tile_rows_force = g0.force_rows;
   }
   info->horizon_ms = s.horizon_ms;
   info->horizon_on_gpu = s.horizon_on_gpu;
@@ -1463,7 +1499,7 @@ int lps_profile_kernels(lps_handle *h, int n_steps, int diag_every, lps_kernel_t
       int st = drain_log(h);
       if (st) return st;
     }
-    h->launches += enqueue_step(h, h->step, diag, &mark);
+    h->launches += enqueue_step(h, h->step, diag, r == n_steps - 1, &mark);
     h->step += 1;
     h->pending_records += diag ? 1 : 0;
   }

@@ -39,8 +39,8 @@ constexpr int kTileDeep32 = 2;  // full, and B' = m_ref / m is 1.0f at every own
 
 // FP32-mixed form: per-cell buffers of the dense kernels.
 struct Dense32 {
-  float2 *ab32;           // force coefficients (A', B'), written with theta; 0 at absent cells
-  const float2 *coef32;   // (q, q) with q = m_ref / m_i; (0, -1) where m_i <= 0
+  float *ap32;            // force coefficient A' = dx q (lambda_PD / alpha) theta, written with theta; 0 at absent cells
+  const float *bp32;      // force coefficient B' = q = m_ref / m_i (static); 0 at absent cells and where m_i <= 0
   const float2 *w32;      // W_i = sum over present offsets of beta (a, b)
   const float4 *ka32;     // Ka_i = sum over absent offsets of beta xi_hat xi_hat^T: (xx, xy, yy, 0)
 };
@@ -59,7 +59,7 @@ struct DenseMaps {
   CUtensorMap coef;       // (2(l-m)/m_i, 8 mu/m_i)
   CUtensorMap type;       // u8 node type
   CUtensorMap u32[2];     // FP32-mixed form: FP32 predicted displacements, by step parity
-  CUtensorMap ab32;       // FP32-mixed form: force coefficients (A', B')
+  CUtensorMap ap32, bp32; // FP32-mixed form: force coefficient planes A', B' (one float per cell)
 };
 
 struct DenseGroup {
@@ -69,8 +69,10 @@ struct DenseGroup {
   int grid_theta;   // persistent grid sizes
   int grid_force;
   int theta_rows;   // rows of a dilatation thread: 4 or 2
+  int force_rows;   // rows of a force thread: 2, or 4 (FP32-mixed form)
   int max_theta_ctas, max_force_ctas;  // resident CTAs per SM at full occupancy
   int max_theta_ctas2;                 // the same for the two-row dilatation kernel
+  int max_force_ctas4;                 // the same for the four-row FP32-mixed force kernel
   int *sched;       // device tile-scheduler counters (theta: [0..1], force: [2..3])
   DenseMaps maps;
 };
@@ -105,11 +107,11 @@ void dense_offsets(int m, std::vector<int> &a, std::vector<int> &b);
 // Per-offset FP64 constants of ratio m for lattice spacing dx (= dy) and
 // horizon delta, into __constant__ memory.
 cudaError_t upload_dense_constants(int m, double dx, double dy, double delta, cudaStream_t st);
-// Encodes the TMA descriptors of group g over the given buffers (U32 and
-// ab32 only in the FP32-mixed form, else null).
+// Encodes the TMA descriptors of group g over the given buffers (U32, ap32
+// and bp32 only in the FP32-mixed form, else null).
 int dense_encode_maps(DenseGroup &g, int pitch, int total_rows, double2 *const *U, double *const *TH,
-                      const double2 *coef, const uint8_t *type, float2 *const *U32, const float2 *ab32,
-                      std::string &err);
+                      const double2 *coef, const uint8_t *type, float2 *const *U32, const float *ap32,
+                      const float *bp32, std::string &err);
 // FP32-mixed form, host side: W_i and Ka_i of the existing cells in
 // [first, first + count) of an m-stencil grid, and whether a tile whose first
 // owned cell is first_owned is deep (kTileDeep32).
@@ -119,9 +121,10 @@ bool dense32_tile_deep(int m, const std::vector<uint8_t> &type, const std::vecto
                        long first_owned);
 // Sets shared-memory limits and the persistent grid sizes of each group.
 cudaError_t dense_prepare(DenseGeo &dg);
-// Persistent grids of every group at the given resident CTAs per SM (each
-// clamped to 1..the group's occupancy limit).
-void dense_set_ctas(DenseGeo &dg, int theta_rows, int theta_ctas, int force_ctas);
+// Persistent grids of every group at the given rows per thread and resident
+// CTAs per SM (each clamped to 1..the group's occupancy limit); force_rows 4
+// only in the FP32-mixed form.
+void dense_set_ctas(DenseGeo &dg, int theta_rows, int theta_ctas, int force_ctas, int force_rows = 2);
 
 // FP32-mixed tile kernels (lps_kernels_dense32.cu): shared-memory limits,
 // persistent grids and launches of one group.

@@ -31,6 +31,9 @@ constexpr int kAbcWarpsPerBlock = 8; // warps per ABC block (one ABC node each)
 constexpr uint8_t kExists = 1;       // a real node (not padding)
 constexpr uint8_t kBcAbc = 2;        // BCTypes[2i] == 1 (IDW skips these, :778)
 constexpr uint8_t kActiveAbc = 4;    // overwritten by the G operators this step
+constexpr uint8_t kKeepState = 8;    // read every step by the absorbing-boundary kernels (a cloud entry of
+                                     // a writing ABC node, or an IDW neighbour): its v and theta are
+                                     // written on every step, not only on full steps (StepPtrs::full)
 
 // Per-instance constants, one device table per handle (Geo::ip, Abc::ip),
 // indexed by instance id.
@@ -45,6 +48,7 @@ struct InstParams {
   double out_r;     // energy exclusion radius, <= 0: none (:528-530)
   double f32_b0;    // FP32-mixed form: force scale alpha = 8 mu / m_ref (:485)
   double f32_ab;    // FP32-mixed form: lambda_PD / alpha = (lambda - mu) / (4 mu)
+  double mref;      // m_ref = max m_i (:429-442): m_i of every full-horizon node
   int node_begin, node_count;   // global node (or cell) range
   int abc_begin, abc_count;     // packed ABC list range
   int n_active_abc;             // entries with BCTypes == 1 (uB/vB denominators)
@@ -75,7 +79,10 @@ struct StepPtrs {
   float2 *u32_np1;         // FP32-mixed form: FP32 copy of the predicted u^{n+1}
   float2 *u32_np2;         // FP32-mixed form: FP32 copy of u^{n+2}, written by the force pass
   int th_ring;             // ring index of th_np1
-  int pad;
+  int full;                // dense path: 1 = write v, a and theta at every node; 0 = only where a
+                           // later step reads them (kKeepState and ABC nodes).  Diagnostic steps
+                           // and the last step of every lps_step call are full, so whatever the
+                           // diagnostics or lps_download read is current.
 };
 
 // Geometry + static per-node data.

@@ -27,7 +27,7 @@ void launch_predict_csr(const LaunchGeo &g, const StepPtrs &p, cudaStream_t st);
 void launch_theta_csr(const LaunchGeo &g, const double2 *u, double *theta, const double *th_n,
                       const double *th_nm1, bool abc_override, cudaStream_t st);
 void launch_theta_idw(const LaunchGeo &g, double *theta, cudaStream_t st, float2 *ab32 = nullptr,
-                      const float2 *coef32 = nullptr);
+                      const float2 *coef32 = nullptr, float *ap32 = nullptr, const float *bp32 = nullptr);
 void launch_force_csr(const LaunchGeo &g, const StepPtrs &p, int *d_step, cudaStream_t st);
 
 // CSR path, FP32-mixed form (lps_kernels_csr32.cu): the predictor above also

@@ -78,9 +78,11 @@ __global__ void __launch_bounds__(kNodeBlock)
 // Inverse-distance-weighted theta at ABC nodes, src/main.cpp:765-790.  The
 // neighbour lists and weights w = 1/(|r| + 1e-30) are built on the host in the
 // reference's horizon order.  Runs after the dilatation pass (needs current
-// theta); in the FP32-mixed form it also writes the nodes' force coefficients.
+// theta); in the FP32-mixed form it also writes the nodes' force coefficients:
+// (A', B') pairs on the neighbour-list path (ab32), the A' plane on the dense
+// path (ap32, from the static B' plane bp32).
 __global__ void __launch_bounds__(kNodeBlock)
-    k_theta_idw(Abc ab, double *theta, float2 *ab32, const float2 *coef32) {
+    k_theta_idw(Abc ab, double *theta, float2 *ab32, const float2 *coef32, float *ap32, const float *bp32) {
   const int a = blockIdx.x * kAbcWarpsPerBlock + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (a >= ab.n_abc || !ab.writes[a]) return;
@@ -97,6 +99,7 @@ __global__ void __launch_bounds__(kNodeBlock)
   if (lane == 0 && ws > 0.0) {
     theta[ab.node[a]] = ta / ws;
     if (ab32) write_ab32(ab32, coef32, ab.node[a], ta / ws, ab.ip[ab.inst[a]]);
+    if (ap32) write_ap32(ap32, bp32, ab.node[a], ta / ws, ab.ip[ab.inst[a]]);
   }
 }
 
@@ -227,9 +230,10 @@ void launch_theta_csr(const LaunchGeo &g, const double2 *u, double *theta, const
                                               gth ? 1 : 0);
 }
 
-void launch_theta_idw(const LaunchGeo &g, double *theta, cudaStream_t st, float2 *ab32, const float2 *coef32) {
+void launch_theta_idw(const LaunchGeo &g, double *theta, cudaStream_t st, float2 *ab32, const float2 *coef32,
+                      float *ap32, const float *bp32) {
   if (g.abc.n_abc == 0) return;
-  k_theta_idw<<<g.n_abc_blocks, kNodeBlock, 0, st>>>(g.abc, theta, ab32, coef32);
+  k_theta_idw<<<g.n_abc_blocks, kNodeBlock, 0, st>>>(g.abc, theta, ab32, coef32, ap32, bp32);
 }
 
 void launch_force_csr(const LaunchGeo &g, const StepPtrs &p, int *d_step, cudaStream_t st) {

@@ -344,7 +344,7 @@ __global__ void __launch_bounds__(kTileThreads, 2)
       const size_t cell = cell0 + (size_t)k * pitch;
       const bool valid = sab[QI<M>(r0 + k, lane)].y > 0.0;  // m_i > 0 (:827-831)
       const double2 acc = valid ? make_double2(F[k].x / P.rho, F[k].y / P.rho) : make_double2(0.0, 0.0);
-      p.a_np1[cell] = acc;
+      if (p.full || (ty & (kKeepState | kActiveAbc))) p.a_np1[cell] = acc;
       if (abc_on && (ty & kActiveAbc)) continue;  // G_v writes v; the next theta kernel predicts u
       // corrector (:924) then the next predictor (:727) from the same values
       const double2 vh = k == 0 ? vh0 : vh1;
@@ -356,7 +356,7 @@ __global__ void __launch_bounds__(kTileThreads, 2)
       const double2 u = su[QI<M>(r0 + k, lane)];
       un.x = u.x + P.dt * vh2.x;
       un.y = u.y + P.dt * vh2.y;
-      p.v_np1[cell] = v;
+      if (p.full || (ty & kKeepState)) p.v_np1[cell] = v;
       p.vh[cell] = vh2;
       p.u_np2[cell] = un;
     }
@@ -676,6 +676,8 @@ static cudaError_t prepare_m(DenseGroup &gr, int n_sm) {
   gr.max_theta_ctas = bt;
   gr.max_theta_ctas2 = std::max(bt2, 1);
   gr.max_force_ctas = bf;
+  gr.force_rows = 2;
+  gr.max_force_ctas4 = 0;  // the FP64 force pass has the two-row form only
   return cudaSuccess;
 }
 
@@ -684,14 +686,15 @@ static void prepare_dispatch(DenseGroup &gr, int n_sm, cudaError_t *e) {
   *e = prepare_m<M>(gr, n_sm);
 }
 
-void dense_set_ctas(DenseGeo &dg, int theta_rows, int theta_ctas, int force_ctas) {
+void dense_set_ctas(DenseGeo &dg, int theta_rows, int theta_ctas, int force_ctas, int force_rows) {
   int dev = 0, n_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
   for (auto &gr : dg.groups) {
     gr.theta_rows = theta_rows == 2 ? 2 : 4;
+    gr.force_rows = (force_rows == 4 && gr.max_force_ctas4 > 0) ? 4 : 2;
     const int t = std::max(1, std::min(theta_ctas, gr.theta_rows == 2 ? gr.max_theta_ctas2 : gr.max_theta_ctas));
-    const int f = std::max(1, std::min(force_ctas, gr.max_force_ctas));
+    const int f = std::max(1, std::min(force_ctas, gr.force_rows == 4 ? gr.max_force_ctas4 : gr.max_force_ctas));
     gr.grid_theta = std::min(gr.n_tiles, t * n_sm);
     gr.grid_force = std::min(gr.n_tiles, f * n_sm);
   }
@@ -742,14 +745,17 @@ bool encode(CUtensorMap *map, CUtensorMapDataType dt, size_t elem, const void *b
 
 template <int M>
 void encode_m(DenseGroup &g, int pitch, int rows, double2 *const *U, double *const *TH, const double2 *coef,
-              const uint8_t *type, float2 *const *U32, const float2 *ab32, bool *ok) {
+              const uint8_t *type, float2 *const *U32, const float *ap32, const float *bp32, bool *ok) {
   using R = Region<M>;
   bool good = true;
   if (U32) {
+    // FP32-mixed planes; the coefficient boxes are RC rounded up to 16 bytes
+    const uint32_t rca = (R::RC + 3) / 4 * 4;
     for (int r = 0; r < 2; r++)
       good &= encode(&g.maps.u32[r], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, U32[r], 2ull * pitch, rows, 2 * R::RC,
                      R::RR);
-    good &= encode(&g.maps.ab32, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, ab32, 2ull * pitch, rows, 2 * R::RC, R::RR);
+    good &= encode(&g.maps.ap32, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, ap32, pitch, rows, rca, R::RR);
+    good &= encode(&g.maps.bp32, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, bp32, pitch, rows, rca, R::RR);
   }
   for (int r = 0; r < kUring; r++)
     good &= encode(&g.maps.u[r], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, U[r], 2ull * pitch, rows, 2 * R::RC, R::RR);
@@ -762,10 +768,10 @@ void encode_m(DenseGroup &g, int pitch, int rows, double2 *const *U, double *con
 }  // namespace
 
 int dense_encode_maps(DenseGroup &g, int pitch, int total_rows, double2 *const *U, double *const *TH,
-                      const double2 *coef, const uint8_t *type, float2 *const *U32, const float2 *ab32,
-                      std::string &err) {
+                      const double2 *coef, const uint8_t *type, float2 *const *U32, const float *ap32,
+                      const float *bp32, std::string &err) {
   bool ok = false;
-  LPS_DISPATCH_M(g.m, encode_m, g, pitch, total_rows, U, TH, coef, type, U32, ab32, &ok);
+  LPS_DISPATCH_M(g.m, encode_m, g, pitch, total_rows, U, TH, coef, type, U32, ap32, bp32, &ok);
   if (!ok) {
     err = "cuTensorMapEncodeTiled failed for the dense layout";
     return LPS_ERR_CUDA;
@@ -834,7 +840,7 @@ int enqueue_dense_step(const DenseGeo &dg, const LaunchGeo &lg, const StepPtrs &
   }
   if (mark) (*mark)("theta_tiles");
   if (abc && lg.theta_method == 0) {
-    launch_theta_idw(lg, p.th_np1, st, dg.fp32 ? dg.d32.ab32 : nullptr, dg.d32.coef32);
+    launch_theta_idw(lg, p.th_np1, st, nullptr, nullptr, dg.fp32 ? dg.d32.ap32 : nullptr, dg.d32.bp32);
     if (mark) (*mark)("theta_idw");
     k++;
   }

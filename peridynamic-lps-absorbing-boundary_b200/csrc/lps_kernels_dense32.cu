@@ -4,8 +4,8 @@
 // the bond arithmetic in FP32:
 //   k_theta32<M,K>  dilatation (src/main.cpp:736-761) from an FP32 copy of the
 //                   predicted displacements; its epilogue also writes the force
-//                   pass's per-cell coefficients (A', B') in FP32
-//   k_force32<M>    force (:821-874) in FP32; corrector (:922-925) and the
+//                   pass's per-cell coefficient A' (B' is static)
+//   k_force32<M,K>  force (:821-874) in FP32; corrector (:922-925) and the
 //                   next predictor (:725-728) in FP64, which also writes the
 //                   FP32 copy of the next predicted level
 // Kept in FP64: the displacement / velocity / acceleration state and its
@@ -66,22 +66,34 @@ __host__ __device__ constexpr double sten_qd(int Q, int M, int a, int b) {
 __host__ __device__ constexpr float sten_q(int Q, int M, int a, int b) { return (float)sten_qd(Q, M, a, b); }
 
 // Staged-region geometry of the FP32 tile kernels: the dilatation stages the
-// FP32 displacements, the force pass the displacements and (A', B').
+// FP32 displacements, the force pass the displacements and the coefficient
+// planes A' and B' (one float per cell; B' only for tiles that are not deep).
+// The planes' staged rows are RCA floats wide, RC rounded up to 16 bytes, as a
+// TMA box's inner extent must be.
 template <int M>
 struct Region32 {
   static constexpr int RR = kTileRows + 2 * M;
   static constexpr int RC = kTileCols + 2 * M;
+  static constexpr int RCA = (RC + 3) / 4 * 4;
   static constexpr int CELLS = RR * RC;
   static constexpr int align128(int x) { return (x + 127) / 128 * 128; }
   static constexpr int U_BYTES = CELLS * 8;
+  static constexpr int P_BYTES = RR * RCA * 4;
   static constexpr int THETA_STAGE = align128(U_BYTES);
   static constexpr int THETA_TX = U_BYTES;
-  static constexpr int F_AB = align128(U_BYTES);
-  static constexpr int FORCE_STAGE = align128(F_AB + CELLS * 8);
-  static constexpr int FORCE_TX = 2 * CELLS * 8;
+  static constexpr int F_A = align128(U_BYTES);
+  static constexpr int F_B = align128(F_A + P_BYTES);
+  static constexpr int FORCE_STAGE = align128(F_B + P_BYTES);
+  static constexpr int FORCE_TX_DEEP = U_BYTES + P_BYTES;
+  static constexpr int FORCE_TX = U_BYTES + 2 * P_BYTES;
   static constexpr int THETA_SMEM = 2 * THETA_STAGE + 64;
   static constexpr int FORCE_SMEM = 2 * FORCE_STAGE + 64;
 };
+// staged coefficient-plane index of tile-relative cell (r, c)
+template <int M>
+__device__ __forceinline__ int QA(int r, int c) {
+  return (r + M) * Region32<M>::RCA + (c + M);
+}
 
 // Two FP32 values in one 64-bit register pair, for Blackwell's paired FP32
 // instructions (add/sub/fma .f32x2: one instruction for the x and y parts).
@@ -117,6 +129,14 @@ __device__ __forceinline__ void kahan_add(float &s, float &c, float x) {
   const float y = x - c;
   const float t = s + y;
   c = (t - s) - y;
+  s = t;
+}
+
+// The same for an (x, y) pair in paired instructions (each lane as kahan_add).
+__device__ __forceinline__ void kahan_add2(f32x2 &s, f32x2 &c, f32x2 x) {
+  const f32x2 y = f2_sub(x, c);
+  const f32x2 t = f2_add(s, y);
+  c = f2_sub(f2_sub(t, s), y);
   s = t;
 }
 
@@ -162,64 +182,100 @@ __device__ __forceinline__ void theta_tile32(const float2 *__restrict__ su, int 
   for (int k = 0; k < K; k++) th[k] = S[k] - C[k];
 }
 
-// Force sums of cells (r0, c), (r0 + 1, c).  DEEP: every coefficient B' is 1
+// Force sums of cells (r0 + k, c), k < K.  DEEP: every coefficient B' is 1
 // (folded form); otherwise the general pair form, whose absent-neighbour terms
-// the caller corrects.
-template <int M, bool DEEP>
-__device__ __forceinline__ void force_tile32(const float2 *__restrict__ su, const float2 *__restrict__ sab, int r0,
-                                             int c, float F[2][2]) {
+// the caller corrects.  Column by column (stencil offset b), the thread walks
+// the pairs (a, b) / (-a, -b) in order of a and keeps two sliding windows of K
+// staged cells: rows r0 + a + k of column c + b and rows r0 - a + k of column
+// c - b.  Each step of a moves both windows by one row, so every staged value
+// is loaded once per column and feeds up to K cells from registers.
+template <int M, int K, bool DEEP>
+__device__ __forceinline__ void force_tile32(const float2 *__restrict__ su, const float *__restrict__ sa,
+                                             const float *__restrict__ sb, int r0, int c, float F[K][2]) {
   const f32x2 *__restrict__ sp = reinterpret_cast<const f32x2 *>(su);
-  f32x2 ui[2];
-  float bi[2];
-  float S0[2] = {0.f, 0.f}, C0[2] = {0.f, 0.f}, S1[2] = {0.f, 0.f}, C1[2] = {0.f, 0.f};
-  float p0[2] = {0.f, 0.f}, p1[2] = {0.f, 0.f};
+  f32x2 ui[K], S[K], Cc[K];
+  float bi[K];
 #pragma unroll
-  for (int k = 0; k < 2; k++) {
+  for (int k = 0; k < K; k++) {
     ui[k] = sp[QI<M>(r0 + k, c)];
-    bi[k] = sab[QI<M>(r0 + k, c)].y;
+    bi[k] = DEEP ? 1.f : sb[QA<M>(r0 + k, c)];
+    S[k] = Cc[k] = 0ull;
   }
   const f32x2 m2 = f2_pack(-2.f, -2.f);
-  for_each_pair<M>(
-      [&](auto ac, auto bc) {
-        constexpr int a = decltype(ac)::value, b = decltype(bc)::value;
-        constexpr float hx = sten_q(kHx, M, a, b), hy = sten_q(kHy, M, a, b), L = sten_q(kR, M, a, b);
-        constexpr float gx = sten_q(kGx, M, a, b), gy = sten_q(kGy, M, a, b);
+  static_for<0, M + 1>([&](auto bc) {
+    constexpr int b = decltype(bc)::value;
+    constexpr int A = amax(M, b);
+    constexpr int a0 = b == 0 ? 1 : -A;  // b = 0: pairs (a, 0) with a > 0
+    f32x2 wp[K], wm[K];                  // u at rows r0 + a + k (column c + b), r0 - a + k (column c - b)
+    float ap[K], am[K], bp[K], bm[K];    // A', B' there
+    float p0[K], p1[K];
 #pragma unroll
-        for (int k = 0; k < 2; k++) {
-          const int r = r0 + k;
-          const int qp = QI<M>(r + a, c + b), qm = QI<M>(r - a, c - b);
-          float T;
-          if (DEEP) {
-            // 2 xi_hat . (u(+) + u(-) - 2 u_i) + (A'+ - A'-) r
-            const float2 s = f2_unpack(f2_fma(m2, ui[k], f2_add(sp[qp], sp[qm])));
-            const float e = fmaf(2.f * hx, s.x, (2.f * hy) * s.y);
-            T = fmaf(L, sab[qp].x - sab[qm].x, e);
-          } else {
-            const float2 abp = sab[qp], abm = sab[qm];
-            const float2 d1 = f2_unpack(f2_sub(sp[qp], ui[k]));  // u(+) - u_i
-            const float2 d2 = f2_unpack(f2_sub(ui[k], sp[qm]));  // u_i - u(-)
-            const float e1 = fmaf(hx, d1.x, hy * d1.y);
-            const float e2 = fmaf(hx, d2.x, hy * d2.y);
-            T = (abp.x - abm.x) * L;
-            T = fmaf(bi[k] + abp.y, e1, T);
-            T = fmaf(-(bi[k] + abm.y), e2, T);
-          }
-          p0[k] = fmaf(T, gx, p0[k]);
-          p1[k] = fmaf(T, gy, p1[k]);
+    for (int k = 0; k < K; k++) {
+      wp[k] = sp[QI<M>(r0 + a0 + k, c + b)];
+      wm[k] = sp[QI<M>(r0 - a0 + k, c - b)];
+      ap[k] = sa[QA<M>(r0 + a0 + k, c + b)];
+      am[k] = sa[QA<M>(r0 - a0 + k, c - b)];
+      if (!DEEP) {
+        bp[k] = sb[QA<M>(r0 + a0 + k, c + b)];
+        bm[k] = sb[QA<M>(r0 - a0 + k, c - b)];
+      }
+      p0[k] = p1[k] = 0.f;
+    }
+    static_for<a0, A + 1>([&](auto ac) {
+      constexpr int a = decltype(ac)::value;
+      constexpr float hx = sten_q(kHx, M, a, b), hy = sten_q(kHy, M, a, b), L = sten_q(kR, M, a, b);
+      constexpr float gx = sten_q(kGx, M, a, b), gy = sten_q(kGy, M, a, b);
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        float T;
+        if (DEEP) {
+          // 2 xi_hat . (u(+) + u(-) - 2 u_i) + (A'+ - A'-) r
+          const float2 s = f2_unpack(f2_fma(m2, ui[k], f2_add(wp[k], wm[k])));
+          const float e = fmaf(2.f * hx, s.x, (2.f * hy) * s.y);
+          T = fmaf(L, ap[k] - am[k], e);
+        } else {
+          const float2 d1 = f2_unpack(f2_sub(wp[k], ui[k]));  // u(+) - u_i
+          const float2 d2 = f2_unpack(f2_sub(ui[k], wm[k]));  // u_i - u(-)
+          const float e1 = fmaf(hx, d1.x, hy * d1.y);
+          const float e2 = fmaf(hx, d2.x, hy * d2.y);
+          T = (ap[k] - am[k]) * L;
+          T = fmaf(bi[k] + bp[k], e1, T);
+          T = fmaf(-(bi[k] + bm[k]), e2, T);
         }
-      },
-      [&](auto) {
+        p0[k] = fmaf(T, gx, p0[k]);
+        p1[k] = fmaf(T, gy, p1[k]);
+      }
+      if constexpr (a < A) {  // slide: + window down a row, - window up a row
 #pragma unroll
-        for (int k = 0; k < 2; k++) {
-          kahan_add(S0[k], C0[k], p0[k]);
-          kahan_add(S1[k], C1[k], p1[k]);
-          p0[k] = p1[k] = 0.f;
+        for (int k = 0; k + 1 < K; k++) {
+          wp[k] = wp[k + 1];
+          ap[k] = ap[k + 1];
+          if (!DEEP) bp[k] = bp[k + 1];
         }
-      });
 #pragma unroll
-  for (int k = 0; k < 2; k++) {
-    F[k][0] = S0[k] - C0[k];
-    F[k][1] = S1[k] - C1[k];
+        for (int k = K - 1; k > 0; k--) {
+          wm[k] = wm[k - 1];
+          am[k] = am[k - 1];
+          if (!DEEP) bm[k] = bm[k - 1];
+        }
+        wp[K - 1] = sp[QI<M>(r0 + a + K, c + b)];
+        ap[K - 1] = sa[QA<M>(r0 + a + K, c + b)];
+        wm[0] = sp[QI<M>(r0 - a - 1, c - b)];
+        am[0] = sa[QA<M>(r0 - a - 1, c - b)];
+        if (!DEEP) {
+          bp[K - 1] = sb[QA<M>(r0 + a + K, c + b)];
+          bm[0] = sb[QA<M>(r0 - a - 1, c - b)];
+        }
+      }
+    });
+#pragma unroll
+    for (int k = 0; k < K; k++) kahan_add2(S[k], Cc[k], f2_pack(p0[k], p1[k]));
+  });
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    const float2 f = f2_unpack(f2_sub(S[k], Cc[k]));
+    F[k][0] = f.x;
+    F[k][1] = f.y;
   }
 }
 
@@ -264,16 +320,18 @@ __global__ void __launch_bounds__(th32_threads(K), K == 4 ? 6 : 4)
     const float2 *su = reinterpret_cast<const float2 *>(smem + stage * R::THETA_STAGE);
     const int r0 = K * warp;
     const size_t cell0 = (size_t)(t.row + M + r0) * pitch + t.col + M + lane;
-    // the owned cells' static data, fetched while the copy lands
+    // the owned cells' static data, fetched while the copy lands; in a full
+    // tile every owned cell has m_i = m_ref and B' = 1, so only the types
+    const bool full = t.flags & kTileFull;
     double mi[K];
     uint8_t ty[K];
     float q[K];
 #pragma unroll
     for (int k = 0; k < K; k++) {
       const size_t cell = cell0 + (size_t)k * pitch;
-      mi[k] = g.m[cell];
       ty[k] = g.type[cell];
-      q[k] = d32.coef32[cell].y;
+      mi[k] = full ? P.mref : g.m[cell];
+      q[k] = full ? 1.f : d32.bp32[cell];
     }
     const bool landed = mbar_wait_bounded(&bar[stage], (it >> 1) & 1, err);
     if (__syncthreads_or(!landed)) {  // a copy timed out: leave the loop together
@@ -284,7 +342,6 @@ __global__ void __launch_bounds__(th32_threads(K), K == 4 ? 6 : 4)
     theta_tile32<M, K>(su, r0, lane, th);
     const double scale = 2.0 * P.dx * P.dy * P.dx;
     const float dxf = (float)P.dx;
-    const bool full = t.flags & kTileFull;
 #pragma unroll
     for (int k = 0; k < K; k++) {
       if (!(ty[k] & kExists)) continue;
@@ -299,9 +356,9 @@ __global__ void __launch_bounds__(th32_threads(K), K == 4 ? 6 : 4)
           tk -= fmaf(w.x, ui.x, w.y * ui.y);
         }
         thd = (mi[k] > 0.0) ? (scale / mi[k]) * (double)tk : 0.0;
-        p.th_np1[cell] = thd;
+        if (p.full || (ty[k] & kKeepState)) p.th_np1[cell] = thd;  // the force pass reads A'
       }
-      d32.ab32[cell] = q[k] > 0.f ? make_float2((float)(thd * P.f32_ab) * q[k] * dxf, q[k]) : make_float2(0.f, 0.f);
+      d32.ap32[cell] = q[k] > 0.f ? (float)(thd * P.f32_ab) * q[k] * dxf : 0.f;
     }
     fence_proxy_async_smem();
     __syncthreads();  // the stage is refilled at the start of the next-but-one iteration
@@ -313,12 +370,16 @@ __global__ void __launch_bounds__(th32_threads(K), K == 4 ? 6 : 4)
 // ---------------------------------------------------------------------------
 // Force (FP32) + corrector + next predictor (FP64), persistent over tiles.
 // The FP32 sum is F / alpha with alpha = 8 mu / m_ref; the per-instance
-// constants are applied once, in FP64, to the finished sum.
-template <int M>
-__global__ void __launch_bounds__(kTileThreads, 3)
-    k_force32(const __grid_constant__ CUtensorMap map_u, const __grid_constant__ CUtensorMap map_ab, Geo g,
-              const DenseTile *__restrict__ tiles, int tile_begin, int n_tiles, StepPtrs p, Dense32 d32, int pitch,
-              int abc_on, int bump_step, int *d_step, int *sched, int *err) {
+// constants are applied once, in FP64, to the finished sum.  A thread owns K
+// (2 or 4) adjacent rows of one column.  Deep tiles stage u and A' only.
+constexpr int f32_threads(int K) { return kTileRows * kTileCols / K; }
+
+template <int M, int K>
+__global__ void __launch_bounds__(f32_threads(K), K == 4 ? 4 : 3)
+    k_force32(const __grid_constant__ CUtensorMap map_u, const __grid_constant__ CUtensorMap map_a,
+              const __grid_constant__ CUtensorMap map_b, Geo g, const DenseTile *__restrict__ tiles, int tile_begin,
+              int n_tiles, StepPtrs p, Dense32 d32, int pitch, int abc_on, int bump_step, int *d_step, int *sched,
+              int *err) {
   using R = Region32<M>;
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t *bar = reinterpret_cast<uint64_t *>(smem + 2 * R::FORCE_STAGE);
@@ -336,9 +397,11 @@ __global__ void __launch_bounds__(kTileThreads, 3)
   auto issue = [&](int stage, int tile) {
     const DenseTile t = tiles[tile_begin + tile];
     unsigned char *base = smem + stage * R::FORCE_STAGE;
-    mbar_expect_tx(&bar[stage], R::FORCE_TX);
+    const bool deep = t.flags & kTileDeep32;
+    mbar_expect_tx(&bar[stage], deep ? R::FORCE_TX_DEEP : R::FORCE_TX);
     tma_load_2d(base, &map_u, 2 * t.col, t.row, &bar[stage]);
-    tma_load_2d(base + R::F_AB, &map_ab, 2 * t.col, t.row, &bar[stage]);
+    tma_load_2d(base + R::F_A, &map_a, t.col, t.row, &bar[stage]);
+    if (!deep) tma_load_2d(base + R::F_B, &map_b, t.col, t.row, &bar[stage]);
   };
   int tile = s_tile[0];
   if (tid == 0 && tile < n_tiles) issue(0, tile);
@@ -355,53 +418,61 @@ __global__ void __launch_bounds__(kTileThreads, 3)
     const InstParams &P = g.ip[t.inst];
     unsigned char *base = smem + stage * R::FORCE_STAGE;
     const float2 *su = reinterpret_cast<const float2 *>(base);
-    const float2 *sab = reinterpret_cast<const float2 *>(base + R::F_AB);
-    const int r0 = 2 * warp;
+    const float *sa = reinterpret_cast<const float *>(base + R::F_A);
+    const float *sb = reinterpret_cast<const float *>(base + R::F_B);
+    const bool deep = t.flags & kTileDeep32, full = t.flags & kTileFull;
+    const int r0 = K * warp;
     const size_t cell0 = (size_t)(t.row + M + r0) * pitch + t.col + M + lane;
-    // corrector / predictor inputs of the owned cells, fetched while the copy lands
-    const double2 vh0 = p.vh[cell0], vh1 = p.vh[cell0 + pitch];
-    const double2 un0 = p.u_np1[cell0], un1 = p.u_np1[cell0 + pitch];
-    const uint8_t ty0 = g.type[cell0], ty1 = g.type[cell0 + pitch];
+    // corrector / predictor inputs of the owned cells, fetched while the copy
+    // lands (two rows per thread; with four, after the sums, to save registers)
+    constexpr int KP = K == 2 ? 2 : 0;
+    double2 vhp[KP > 0 ? KP : 1], unp[KP > 0 ? KP : 1];
+    uint8_t ty[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) ty[k] = g.type[cell0 + (size_t)k * pitch];
+#pragma unroll
+    for (int k = 0; k < KP; k++) {
+      vhp[k] = p.vh[cell0 + (size_t)k * pitch];
+      unp[k] = p.u_np1[cell0 + (size_t)k * pitch];
+    }
     const bool landed = mbar_wait_bounded(&bar[stage], (it >> 1) & 1, err);
     if (__syncthreads_or(!landed)) {  // a copy timed out: leave the loop together
       failed = true;
       break;
     }
-    float F[2][2];
-    if (t.flags & kTileDeep32)
-      force_tile32<M, true>(su, sab, r0, lane, F);
+    float F[K][2];
+    if (deep)
+      force_tile32<M, K, true>(su, sa, sb, r0, lane, F);
     else
-      force_tile32<M, false>(su, sab, r0, lane, F);
+      force_tile32<M, K, false>(su, sa, sb, r0, lane, F);
     const double scale = P.f32_b0 * P.dx * P.dy / P.rho;
-    const bool full = t.flags & kTileFull;
 #pragma unroll
-    for (int k = 0; k < 2; k++) {
-      const uint8_t ty = k == 0 ? ty0 : ty1;
-      if (!(ty & kExists)) continue;
+    for (int k = 0; k < K; k++) {
+      if (!(ty[k] & kExists)) continue;
       const size_t cell = cell0 + (size_t)k * pitch;
-      const float2 abi = sab[QI<M>(r0 + k, lane)];
+      const float ai = sa[QA<M>(r0 + k, lane)], bi = deep ? 1.f : sb[QA<M>(r0 + k, lane)];
       if (!full) {  // absent neighbours: A'_i W_i + B'_i Ka_i u_i
         const float2 w = d32.w32[cell], ui = su[QI<M>(r0 + k, lane)];
         const float4 ka = d32.ka32[cell];
-        F[k][0] += fmaf(abi.x, w.x, abi.y * fmaf(ka.x, ui.x, ka.y * ui.y));
-        F[k][1] += fmaf(abi.x, w.y, abi.y * fmaf(ka.y, ui.x, ka.z * ui.y));
+        F[k][0] += fmaf(ai, w.x, bi * fmaf(ka.x, ui.x, ka.y * ui.y));
+        F[k][1] += fmaf(ai, w.y, bi * fmaf(ka.y, ui.x, ka.z * ui.y));
       }
-      const bool valid = abi.y > 0.f;  // m_i > 0 (:827-831)
+      const bool valid = bi > 0.f;  // m_i > 0 (:827-831)
       const double2 acc =
           valid ? make_double2((double)F[k][0] * scale, (double)F[k][1] * scale) : make_double2(0.0, 0.0);
-      p.a_np1[cell] = acc;
-      if (abc_on && (ty & kActiveAbc)) continue;  // G_v writes v; the end-of-step kernel predicts u
+      if (p.full || (ty[k] & (kKeepState | kActiveAbc))) p.a_np1[cell] = acc;
+      if (abc_on && (ty[k] & kActiveAbc)) continue;  // G_v writes v; the end-of-step kernel predicts u
       // corrector (:924) then the next predictor (:727), FP64
-      const double2 vh = k == 0 ? vh0 : vh1;
+      const double2 vh = KP > 0 ? vhp[k < KP ? k : 0] : p.vh[cell];
+      const double2 u = KP > 0 ? unp[k < KP ? k : 0] : p.u_np1[cell];
       double2 v, vh2, un;
       v.x = vh.x + P.half_dt * acc.x;
       v.y = vh.y + P.half_dt * acc.y;
       vh2.x = v.x + P.half_dt * acc.x;
       vh2.y = v.y + P.half_dt * acc.y;
-      const double2 u = k == 0 ? un0 : un1;
       un.x = u.x + P.dt * vh2.x;
       un.y = u.y + P.dt * vh2.y;
-      p.v_np1[cell] = v;
+      if (p.full || (ty[k] & kKeepState)) p.v_np1[cell] = v;
       p.vh[cell] = vh2;
       p.u_np2[cell] = un;
       p.u32_np2[cell] = make_float2((float)un.x, (float)un.y);
@@ -493,33 +564,36 @@ static void prepare32_m(DenseGroup &gr, int n_sm, cudaError_t *out) {
   using R = Region32<M>;
   cudaError_t e;
   *out = cudaSuccess;
-  if ((e = cudaFuncSetAttribute(k_theta32<M, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, R::THETA_SMEM)) ||
-      (e = cudaFuncSetAttribute(k_theta32<M, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, R::THETA_SMEM)) ||
-      (e = cudaFuncSetAttribute(k_force32<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, R::FORCE_SMEM)) ||
-      (e = cudaFuncSetAttribute(k_theta32<M, 4>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                cudaSharedmemCarveoutMaxShared)) ||
-      (e = cudaFuncSetAttribute(k_theta32<M, 2>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                cudaSharedmemCarveoutMaxShared)) ||
-      (e = cudaFuncSetAttribute(k_force32<M>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                cudaSharedmemCarveoutMaxShared))) {
+  const auto smem = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  const auto carve = cudaFuncAttributePreferredSharedMemoryCarveout;
+  const int maxs = cudaSharedmemCarveoutMaxShared;
+  if ((e = cudaFuncSetAttribute(k_theta32<M, 4>, smem, R::THETA_SMEM)) ||
+      (e = cudaFuncSetAttribute(k_theta32<M, 2>, smem, R::THETA_SMEM)) ||
+      (e = cudaFuncSetAttribute(k_force32<M, 2>, smem, R::FORCE_SMEM)) ||
+      (e = cudaFuncSetAttribute(k_force32<M, 4>, smem, R::FORCE_SMEM)) ||
+      (e = cudaFuncSetAttribute(k_theta32<M, 4>, carve, maxs)) || (e = cudaFuncSetAttribute(k_theta32<M, 2>, carve, maxs)) ||
+      (e = cudaFuncSetAttribute(k_force32<M, 2>, carve, maxs)) || (e = cudaFuncSetAttribute(k_force32<M, 4>, carve, maxs))) {
     *out = e;
     return;
   }
-  int bt = 0, bt2 = 0, bf = 0;
+  int bt = 0, bt2 = 0, bf = 0, bf4 = 0;
   if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, k_theta32<M, 4>, th32_threads(4), R::THETA_SMEM)) ||
       (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt2, k_theta32<M, 2>, th32_threads(2), R::THETA_SMEM)) ||
-      (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf, k_force32<M>, kTileThreads, R::FORCE_SMEM))) {
+      (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf, k_force32<M, 2>, f32_threads(2), R::FORCE_SMEM)) ||
+      (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf4, k_force32<M, 4>, f32_threads(4), R::FORCE_SMEM))) {
     *out = e;
     return;
   }
   bt = std::max(bt, 1);
   bf = std::max(bf, 1);
   gr.theta_rows = 4;
+  gr.force_rows = 2;
   gr.grid_theta = std::min(gr.n_tiles, bt * n_sm);
   gr.grid_force = std::min(gr.n_tiles, bf * n_sm);
   gr.max_theta_ctas = bt;
   gr.max_theta_ctas2 = std::max(bt2, 1);
   gr.max_force_ctas = bf;
+  gr.max_force_ctas4 = std::max(bf4, 1);
 }
 
 cudaError_t dense32_prepare_group(DenseGroup &gr, int n_sm) {
@@ -554,12 +628,21 @@ static void theta32_m(const DenseGroup &gr, const LaunchGeo &lg, const DenseGeo 
     theta32_k<M, 4>(gr, lg, dg, p, ring_u, skip_abc, st);
 }
 
+template <int M, int K>
+static void force32_k(const DenseGroup &gr, const LaunchGeo &lg, const DenseGeo &dg, const StepPtrs &p, int ring_u,
+                      bool abc_on, bool first, int *d_step, cudaStream_t st) {
+  k_force32<M, K><<<gr.grid_force, f32_threads(K), Region32<M>::FORCE_SMEM, st>>>(
+      gr.maps.u32[ring_u & 1], gr.maps.ap32, gr.maps.bp32, lg.geo, dg.tiles, gr.tile_begin, gr.n_tiles, p, dg.d32,
+      dg.pitch, abc_on ? 1 : 0, first ? 1 : 0, d_step, gr.sched + 2, dg.d_err);
+}
+
 template <int M>
 static void force32_m(const DenseGroup &gr, const LaunchGeo &lg, const DenseGeo &dg, const StepPtrs &p,
                       int ring_u, int, bool abc_on, bool first, int *d_step, cudaStream_t st) {
-  k_force32<M><<<gr.grid_force, kTileThreads, Region32<M>::FORCE_SMEM, st>>>(
-      gr.maps.u32[ring_u & 1], gr.maps.ab32, lg.geo, dg.tiles, gr.tile_begin, gr.n_tiles, p, dg.d32, dg.pitch,
-      abc_on ? 1 : 0, first ? 1 : 0, d_step, gr.sched + 2, dg.d_err);
+  if (gr.force_rows == 4)
+    force32_k<M, 4>(gr, lg, dg, p, ring_u, abc_on, first, d_step, st);
+  else
+    force32_k<M, 2>(gr, lg, dg, p, ring_u, abc_on, first, d_step, st);
 }
 
 void launch_theta32_group(const DenseGroup &gr, const LaunchGeo &lg, const DenseGeo &dg, const StepPtrs &p,

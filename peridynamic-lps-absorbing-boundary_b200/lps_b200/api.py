@@ -50,7 +50,7 @@ class _Options(C.Structure):
                 ("max_horizon", C.c_int32), ("precision", C.c_int32), ("path", C.c_int32),
                 ("device", C.c_int32), ("use_graphs", C.c_int32), ("stream", C.c_void_p),
                 ("autotune", C.c_int32), ("theta_rows", C.c_int32), ("horizon_build", C.c_int32),
-                ("pad", C.c_int32)]
+                ("force_rows", C.c_int32)]
 
 
 DIAG_FIELDS = ("t", "E", "Ek", "Ep", "Px", "Py", "max_u", "max_v", "max_a",
@@ -76,7 +76,7 @@ class _Info(C.Structure):
                 ("output_exclude_r", C.c_double), ("domain_radius", C.c_double), ("dt_lps", C.c_double),
                 ("device_bytes", C.c_int64), ("step", C.c_int64), ("n_abc_m_corrected", C.c_int32),
                 ("pad", C.c_int32), ("tile_ctas_theta", C.c_int32), ("tile_ctas_force", C.c_int32),
-                ("tile_rows_theta", C.c_int32), ("pad2", C.c_int32), ("horizon_ms", C.c_double),
+                ("tile_rows_theta", C.c_int32), ("tile_rows_force", C.c_int32), ("horizon_ms", C.c_double),
                 ("horizon_on_gpu", C.c_int32), ("pad3", C.c_int32)]
 
 
@@ -143,7 +143,7 @@ class Solver:
                  theta_method: int = 1, kinematic_v: int = 0, max_horizon: int = 128,
                  precision: str = "fp64", path: str = "auto", device: int = 0,
                  use_graphs: bool = True, stream: int | None = None, autotune: bool = False,
-                 theta_rows: int = 0, horizon_build: str = "auto"):
+                 theta_rows: int = 0, horizon_build: str = "auto", force_rows: int = 0):
         lib = load_library()
         if isinstance(problems, InputSet):
             problems = [problems]
@@ -177,6 +177,7 @@ class Solver:
         o.stream = stream
         o.autotune = int(autotune)
         o.theta_rows = int(theta_rows)
+        o.force_rows = int(force_rows)
         o.horizon_build = {"auto": 0, "host": 1, "gpu": 2}[horizon_build]
         h = C.c_void_p()
         st = lib.lps_create(arr, len(self.sets), C.byref(o), C.byref(h))

@@ -106,13 +106,24 @@ def test_batch_equals_single(path):
 
 
 @pytest.mark.parametrize("path", PATHS)
-def test_graphs_match_eager(path):
-    s = gen.disc_problem(R=15.0, m=4, nu=0.35, n_steps=37, sigma=3.0)
-    d1, st1, _, _ = run_gpu(s, path, diag_every=5)
-    d2, st2, _, _ = run_gpu(s, path, diag_every=5, use_graphs=False)
+@pytest.mark.parametrize("n_steps,diag_every", [(37, 5), (24, 0)])
+def test_graphs_match_eager(path, n_steps, diag_every):
+    """Captured graphs give the eager steps' bits.  With 24 steps and no
+    diagnostics the call ends on the last step of a graph, which must leave v,
+    a and theta current at every node (the dense path writes them at interior
+    nodes only on such full steps)."""
+    s = gen.disc_problem(R=15.0, m=4, nu=0.35, n_steps=n_steps, sigma=3.0)
+    d1, st1, _, _ = run_gpu(s, path, diag_every=diag_every)
+    d2, st2, _, _ = run_gpu(s, path, diag_every=diag_every, use_graphs=False)
     for key in ("u", "v", "a", "theta"):
         np.testing.assert_array_equal(st1[key], st2[key])
-    np.testing.assert_array_equal(d1["E"], d2["E"])
+    if diag_every:
+        np.testing.assert_array_equal(d1["E"], d2["E"])
+    else:
+        # against a run with diagnostics every step (all steps full)
+        d3, st3, _, _ = run_gpu(s, path, diag_every=1)
+        for key in ("u", "v", "a", "theta"):
+            np.testing.assert_array_equal(st1[key], st3[key])
 
 
 def test_reset_and_set_initial_repeat():
@@ -157,9 +168,10 @@ def test_horizon_overflow_is_an_error():
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32_mixed"])
 def test_autotune_changes_no_result(precision):
-    """The autotuner only picks rows per dilatation thread and resident CTAs
-    per SM for the tile kernels: every result is the same bits as with the
-    defaults, and so is a run fixed at two rows per dilatation thread."""
+    """The autotuner only picks rows per thread and resident CTAs per SM for
+    the tile kernels: every result is the same bits as with the defaults, and
+    so is a run fixed at two rows per dilatation thread or (FP32-mixed) four
+    rows per force thread."""
     sets = [gen.disc_problem(R=14.0, m=4, nu=0.3, n_steps=40, sigma=3.0),
             gen.disc_problem(R=11.0, m=3, nu=0.2, n_steps=40, sigma=2.5)]
     out = {}
@@ -175,7 +187,15 @@ def test_autotune_changes_no_result(precision):
         assert sv.info(0)["tile_rows_theta"] == 2
         sv.step(40, diag_every=10)
         out["rows2"] = [(sv.read_diag(k), sv.download(k)) for k in range(len(sets))]
-    for other in (True, "rows2"):
+    others = [True, "rows2"]
+    if precision == "fp32_mixed":
+        # four rows per force thread (the FP32-mixed form's other force kernel)
+        with Solver(sets, precision=precision, force_rows=4) as sv:
+            assert sv.info(0)["tile_rows_force"] == 4
+            sv.step(40, diag_every=10)
+            out["force4"] = [(sv.read_diag(k), sv.download(k)) for k in range(len(sets))]
+        others.append("force4")
+    for other in others:
         for k in range(len(sets)):
             for key in ("u", "v", "a", "theta"):
                 np.testing.assert_array_equal(out[other][k][1][key], out[False][k][1][key])
