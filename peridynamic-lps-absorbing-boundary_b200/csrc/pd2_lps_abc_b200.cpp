@@ -21,9 +21,10 @@
 //   --precision fp64|fp32_mixed   (default fp64)
 //   --path auto|dense|csr         (default auto)
 //   --device D                    CUDA device ordinal
-//   --autotune                    time the dense tile kernels' rows per dilatation
-//                                 thread and CTAs per SM at setup
+//   --autotune                    time the dense tile kernels' rows per thread
+//                                 and CTAs per SM at setup
 //   --theta-rows 2|4              fix the rows per dilatation thread
+//   --force-rows 2|4              fix the rows per FP32-mixed force thread
 //   --no-vtk                      skip the VTK files (energy/verify only)
 //   --sync-output                 write each output step's files before the
 //                                 next steps are enqueued (the reference's order)
@@ -292,6 +293,7 @@ int main(int argc, char **argv) {
     else if (k == "--output-threads") out_threads = std::atoi(next("--output-threads"));
     else if (k == "--autotune") opt.autotune = 1;
     else if (k == "--theta-rows") opt.theta_rows = std::atoi(next("--theta-rows"));
+    else if (k == "--force-rows") opt.force_rows = std::atoi(next("--force-rows"));
     else if (k == "--precision") {
       const std::string v = next("--precision");
       if (v == "fp64") opt.precision = LPS_FP64;

@@ -13,7 +13,9 @@ cores, compared with
 Configurations 2 (7 x 196,321 nodes) and 5 (785,349 nodes, m=8) at their
 full 4000 steps need 10 to 20 minutes of oracle time each, more than the
 default suite allows; they run when LPS_FULL_CONFIGS=1 is set, with the same
-bars.  Each test prints the errors it measured.
+bars.  LPS_CONFIG5_STEPS cuts configuration 5 to fewer steps (its oracle
+run at m=8 costs about 0.2 s per step on 16 cores).  Each test prints the
+errors it measured.
 """
 import os
 
@@ -104,8 +106,9 @@ def test_poisson7_fp32_mixed_vs_oracle():
 
 @full_only
 def test_horizon8_vs_oracle():
-    """Configuration 5 (m=8, 224 neighbours): both kernel paths, both forms."""
-    (s,) = configs.horizon8()
+    """Configuration 5 (m=8, 224 neighbours): both kernel paths, both forms
+    (steps: LPS_CONFIG5_STEPS, default the configuration's 4000)."""
+    (s,) = configs.horizon8(int(os.environ.get("LPS_CONFIG5_STEPS", configs.STEPS["horizon8"])))
     r = O.run(s, substep=DIAG_EVERY, max_horizon=256)
     assert r["status"] == 0
     for path in ("dense", "csr"):
