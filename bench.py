@@ -154,7 +154,7 @@ def cpu_sample(sets, args):
     instance where there is one (else the first), for about 1.2e8
     neighbour-weighted node-steps unless --cpu-sample-steps is given.  An
     instance above CPU_MAX_NODES nodes (the 12.57 M-node domain) is timed on a
-    proxy: a disc of the same dx, horizon, nu and dt with about 785,000 nodes,
+    proxy: a disc of the same dx, horizon, nu and dt with 196,321 nodes (R = 250 dx),
     because the reference's own setup (reading the text files and its k-d tree
     horizon search) takes longer than the whole bench for 12.57 M nodes; its
     time-marching rate per node-step does not depend on the disc's size.

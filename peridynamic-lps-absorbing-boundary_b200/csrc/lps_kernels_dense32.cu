@@ -19,12 +19,6 @@
 //   F_i     = alpha dx^2 sum beta xi_hat [ (A'+ - A'-) r + (B'_i + B'+) e+ - (B'_i + B'-) e- ]
 // with B' = B / alpha = m_ref / m and A' = dx B' (lambda_PD / alpha) theta,
 // alpha = 8 mu / m_ref: material constants stay out of the FP32 arithmetic.
-// With e = xi_hat . d the pair term is w (A'+ - A'-) + C ((B'_i + B'+) d+ -
-// (B'_i + B'-) d-) / 2 with the per-offset coefficients w = beta (a, b) (exact
-// for every interior bond) and C = 2 beta xi_hat xi_hat^T, each one FP64
-// product rounded once to FP32, rather than products of separately rounded
-// xi_hat, |xi| and beta: the rounding of these constants is the same on every
-// step, so it shifts the discrete wave speed and its error grows with time.
 //
 // No per-neighbour existence test.  Absent cells hold u = 0 and A' = B' = 0,
 // so every stencil pair is evaluated the same way, and the terms that an
@@ -35,9 +29,8 @@
 // -- theta_i gets -W_i . u_i, F_i gets A'_i W_i + B'_i Ka_i u_i.  Tiles whose
 // cells and neighbours all have B' = 1 ("deep" tiles, the interior) use
 //   F_i = sum beta xi_hat [ (A'+ - A'-) r + 2 xi_hat . (u(+) + u(-) - 2 u_i) ],
-// the same sum with the coefficients folded (F_i = sum C (u(+) + u(-) - 2 u_i)
-// + w (A'+ - A'-)).  Each stencil column's partial sum is added to the cell's
-// total with Kahan compensation.
+// the same sum with the coefficients folded.  Each stencil column's partial
+// sum is added to the cell's total with Kahan compensation.
 #include <cmath>
 
 #include "lps_common.cuh"
@@ -55,11 +48,10 @@ __host__ __device__ constexpr double ct_sqrt(double x) {
 
 // Per-offset constants in lattice units, evaluated by the compiler for each
 // (a, b) of the unrolled stencil.
-enum StenQ { kHx, kHy, kR, kGx, kGy, kWx, kWy, kCxx, kCxy, kCyy };
+enum StenQ { kHx, kHy, kR, kGx, kGy, kWx, kWy };
 
 __host__ __device__ constexpr double sten_qd(int Q, int M, int a, int b) {
-  const double r2 = (double)(a * a + b * b);
-  const double r = ct_sqrt(r2);
+  const double r = ct_sqrt((double)(a * a + b * b));
   const double beta = r <= M - 0.5 ? 1.0 : (r <= M + 0.5 ? M + 0.5 - r : 0.0);
   switch (Q) {
     case kHx: return a / r;           // xi_hat
@@ -67,11 +59,8 @@ __host__ __device__ constexpr double sten_qd(int Q, int M, int a, int b) {
     case kR: return r;                // |xi| / dx
     case kGx: return beta * a / r;    // beta xi_hat
     case kGy: return beta * b / r;
-    case kWx: return beta * a;        // beta (a, b) = beta xi_hat |xi| / dx
-    case kWy: return beta * b;
-    case kCxx: return 2.0 * beta * a * a / r2;  // 2 beta xi_hat xi_hat^T
-    case kCxy: return 2.0 * beta * a * b / r2;
-    default: return 2.0 * beta * b * b / r2;
+    case kWx: return beta * a;        // beta (a, b)
+    default: return beta * b;
   }
 }
 __host__ __device__ constexpr float sten_q(int Q, int M, int a, int b) { return (float)sten_qd(Q, M, a, b); }
@@ -234,27 +223,27 @@ __device__ __forceinline__ void force_tile32(const float2 *__restrict__ su, cons
     }
     static_for<a0, A + 1>([&](auto ac) {
       constexpr int a = decltype(ac)::value;
-      // the pair's coefficients, each one product rounded once from FP64:
-      // C = 2 beta xi_hat xi_hat^T and w = beta xi_hat |xi| / dx = beta (a, b)
-      constexpr float cxx = sten_q(kCxx, M, a, b), cxy = sten_q(kCxy, M, a, b), cyy = sten_q(kCyy, M, a, b);
-      constexpr float wx = sten_q(kWx, M, a, b), wy = sten_q(kWy, M, a, b);
+      constexpr float hx = sten_q(kHx, M, a, b), hy = sten_q(kHy, M, a, b), L = sten_q(kR, M, a, b);
+      constexpr float gx = sten_q(kGx, M, a, b), gy = sten_q(kGy, M, a, b);
 #pragma unroll
       for (int k = 0; k < K; k++) {
-        const float dA = ap[k] - am[k];
+        float T;
         if (DEEP) {
-          // C (u(+) + u(-) - 2 u_i) + w (A'+ - A'-)
+          // 2 xi_hat . (u(+) + u(-) - 2 u_i) + (A'+ - A'-) r
           const float2 s = f2_unpack(f2_fma(m2, ui[k], f2_add(wp[k], wm[k])));
-          p0[k] = fmaf(cxx, s.x, fmaf(cxy, s.y, fmaf(wx, dA, p0[k])));
-          p1[k] = fmaf(cxy, s.x, fmaf(cyy, s.y, fmaf(wy, dA, p1[k])));
+          const float e = fmaf(2.f * hx, s.x, (2.f * hy) * s.y);
+          T = fmaf(L, ap[k] - am[k], e);
         } else {
-          // C ((B'_i + B'+) (u(+) - u_i) - (B'_i + B'-) (u_i - u(-))) / 2 + w (A'+ - A'-)
           const float2 d1 = f2_unpack(f2_sub(wp[k], ui[k]));  // u(+) - u_i
           const float2 d2 = f2_unpack(f2_sub(ui[k], wm[k]));  // u_i - u(-)
-          const float bpl = 0.5f * (bi[k] + bp[k]), bmi = 0.5f * (bi[k] + bm[k]);
-          const float qx = fmaf(bpl, d1.x, -bmi * d2.x), qy = fmaf(bpl, d1.y, -bmi * d2.y);
-          p0[k] = fmaf(cxx, qx, fmaf(cxy, qy, fmaf(wx, dA, p0[k])));
-          p1[k] = fmaf(cxy, qx, fmaf(cyy, qy, fmaf(wy, dA, p1[k])));
+          const float e1 = fmaf(hx, d1.x, hy * d1.y);
+          const float e2 = fmaf(hx, d2.x, hy * d2.y);
+          T = (ap[k] - am[k]) * L;
+          T = fmaf(bi[k] + bp[k], e1, T);
+          T = fmaf(-(bi[k] + bm[k]), e2, T);
         }
+        p0[k] = fmaf(T, gx, p0[k]);
+        p1[k] = fmaf(T, gy, p1[k]);
       }
       if constexpr (a < A) {  // slide: + window down a row, - window up a row
 #pragma unroll
