@@ -16,8 +16,9 @@ Geometry, absorbing ring and clouds follow the reference preprocessor
 (see ``gen``).  Absorbing operators: the preprocessor's least-squares fit
 (``abc="lsq"``, lps_b200.abcfit) at the time step and wavenumber range its
 stability sweep picks for that disc, read from ``SWEEP`` (the sweep itself
-costs 2-3 minutes per disc on 8 cores; ``python -m lps_b200.configs``
-recomputes the table).  Two configurations differ, for cost:
+costs about ten minutes per R=125 mm disc on 8 cores; ``python -m
+lps_b200.configs`` recomputes the table).  Two configurations differ, for
+cost:
 
 * ``large``: the sweep's sample is every ring node with a truncated cloud,
   about 12,500 at R=500 mm, so its pick is taken from the same sweep on an
@@ -56,14 +57,30 @@ SWEEP_PROXY = {(500.0, 0.25, 4, 0.30): (20.0, 0.25, 4, 0.30)}
 _cache: dict = {}
 
 
+def disc_key(R, dx, m, nu):
+    """The SWEEP key of a disc: (R, dx, m, nu) as floats / int, nu to 6 digits."""
+    return (float(R), float(dx), int(m), round(float(nu), 6))
+
+
+# the discs of the configurations that use least-squares operators
+LSQ_DISCS = ([(125.0, 0.5, 4, nu) for nu in POISSON_NUS] + [(500.0, 0.25, 4, 0.30), (250.0, 0.5, 8, 0.40)])
+
+
+def sweep_pick(R, dx, m, nu):
+    """(dt, delta_kappa * sqrt(c_P)) of a disc from SWEEP (through SWEEP_PROXY),
+    or None when it is not tabulated."""
+    key = disc_key(R, dx, m, nu)
+    return SWEEP.get(SWEEP_PROXY.get(key, key))
+
+
 def lsq_disc(R, dx, m, nu, n_steps, abc="lsq", **kw):
     """gen.disc_problem with the fitted operators at the tabulated sweep pick
     (abc="lsq"), or with the operators ``abc`` names.  Fits are cached in the
     process (the bench builds each configuration more than once)."""
     if abc != "lsq":
         return gen.disc_problem(R=R, dx=dx, m=m, nu=nu, n_steps=n_steps, abc=abc, **kw)
-    key_disc = (float(R), float(dx), int(m), round(float(nu), 6))
-    pick = SWEEP.get(SWEEP_PROXY.get(key_disc, key_disc))
+    key_disc = disc_key(R, dx, m, nu)
+    pick = sweep_pick(R, dx, m, nu)
     if pick is None:
         raise KeyError(f"no sweep pick tabulated for disc {key_disc}: run python -m lps_b200.configs")
     key = (key_disc, n_steps, tuple(sorted(kw.items())))

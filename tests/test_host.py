@@ -61,7 +61,7 @@ def test_example1_geometry_counts():
 
 
 def _declared_symbols():
-    txt = open(os.path.join(ROOT, "include", "lps_cuda.h")).read()
+    txt = "".join(open(os.path.join(ROOT, "include", h)).read() for h in ("lps_cuda.h", "lps_abcfit.h"))
     return sorted(set(re.findall(r"^\s*(?:int|void|const char \*|int64_t)\s*\*?\s*(lps_\w+)\(", txt, re.M)))
 
 
@@ -69,7 +69,7 @@ def test_abi_library_exports_every_declared_symbol():
     from lps_b200 import api
     lib = api.load_library()
     syms = _declared_symbols()
-    assert len(syms) >= 13
+    assert len(syms) >= 14 and "lps_abcfit" in syms
     for name in syms:
         assert hasattr(lib, name), name
     assert set(api.EXPORTED) <= set(syms)
@@ -93,3 +93,26 @@ def test_abi_rejects_bad_theta_rows_before_device():
         Solver(load_inputs("td"), theta_rows=3)
     assert e.value.status == -1
     assert "theta_rows" in str(e.value)
+
+
+def test_abi_rejects_bad_force_rows_before_device():
+    """Rows per FP32-mixed force thread other than 0 (default), 2 or 4 is
+    LPS_ERR_INVALID_ARG, before any device call."""
+    from lps_b200.api import LpsError, Solver
+    with pytest.raises(LpsError) as e:
+        Solver(load_inputs("td"), force_rows=3)
+    assert e.value.status == -1
+    assert "force_rows" in str(e.value)
+
+
+def test_every_least_squares_configuration_has_a_sweep_pick():
+    """Each disc of the configurations built with least-squares operators
+    (Example 1, the Poisson-ratio batch, the 12.57 M-node domain through its
+    R = 20 mm proxy, the m = 8 disc) has a tabulated (dt, delta_kappa) pick,
+    so building a configuration never stops for a missing sweep."""
+    from lps_b200 import configs
+    for disc in configs.LSQ_DISCS:
+        pick = configs.sweep_pick(*disc)
+        assert pick is not None, disc
+        dt, dk = pick
+        assert 1e-9 < dt < 1e-7 and 0.0 < dk <= 5.0, (disc, pick)
