@@ -30,6 +30,9 @@ cost:
 """
 from __future__ import annotations
 
+import os
+import tempfile
+
 import numpy as np
 
 from . import gen
@@ -73,10 +76,56 @@ def sweep_pick(R, dx, m, nu):
     return SWEEP.get(SWEEP_PROXY.get(key, key))
 
 
+# keyword arguments of gen.disc_problem that do not change the operator fit
+_PULSE_KW = {"sigma", "centre", "amplitude", "pulse"}
+
+
+def fit_cache_dir() -> str:
+    """Directory of the operator-fit cache shared by processes on this host:
+    $LPS_FIT_CACHE, else lps_b200_fit_cache under the system temp directory."""
+    return os.environ.get("LPS_FIT_CACHE") or os.path.join(tempfile.gettempdir(), "lps_b200_fit_cache")
+
+
+def _fitted(R, dx, m, nu, n_steps, pick, kw):
+    """gen.disc_problem(abc="lsq") at the tabulated pick, with the fitted
+    operators kept in fit_cache_dir(): the first process to need a disc fits
+    it (holding a lock file, so concurrent processes -- torchrun ranks, the
+    two bench arms -- wait for it instead of fitting again) and the others
+    load the operators.  The geometry, ring and clouds are rebuilt, which is
+    cheap; only the fit is read back."""
+    if set(kw) - _PULSE_KW:   # a fit-relevant option: no sharing
+        return gen.disc_problem(R=R, dx=dx, m=m, nu=nu, n_steps=n_steps, abc="lsq", dt=pick[0],
+                                dk_factor=pick[1], **kw)
+    import fcntl
+    d = fit_cache_dir()
+    os.makedirs(d, exist_ok=True)
+    from .api import LIB_PATH
+    st = os.stat(LIB_PATH)   # entries of another build of the fit are not reused
+    name = (f"disc_R{R!r}_dx{dx!r}_m{m}_nu{round(float(nu), 6)!r}_dt{pick[0]!r}_dk{pick[1]!r}"
+            f"_lib{st.st_size}-{int(st.st_mtime)}")
+    path = os.path.join(d, name + ".npz")
+    with open(os.path.join(d, name + ".lock"), "w") as lock:
+        fcntl.flock(lock, fcntl.LOCK_EX)
+        if os.path.exists(path):
+            z = np.load(path)
+            s = gen.disc_problem(R=R, dx=dx, m=m, nu=nu, n_steps=n_steps, abc="average", dt=pick[0], **kw)
+            if z["gu"].shape == s.gu.shape and z["gtheta"].shape == s.gtheta.shape:
+                s.gu, s.gv, s.gtheta = z["gu"], z["gv"], z["gtheta"]
+                s.fit = {k[4:]: v.item() for k, v in z.items() if k.startswith("fit_")}
+                return s
+        s = gen.disc_problem(R=R, dx=dx, m=m, nu=nu, n_steps=n_steps, abc="lsq", dt=pick[0],
+                             dk_factor=pick[1], **kw)
+        tmp = path + f".{os.getpid()}.tmp.npz"
+        np.savez(tmp, gu=s.gu, gv=s.gv, gtheta=s.gtheta, **{"fit_" + k: np.asarray(v) for k, v in s.fit.items()})
+        os.replace(tmp, path)
+        return s
+
+
 def lsq_disc(R, dx, m, nu, n_steps, abc="lsq", **kw):
     """gen.disc_problem with the fitted operators at the tabulated sweep pick
     (abc="lsq"), or with the operators ``abc`` names.  Fits are cached in the
-    process (the bench builds each configuration more than once)."""
+    process (the bench builds each configuration more than once) and on disk
+    for the other processes of this host (fit_cache_dir)."""
     if abc != "lsq":
         return gen.disc_problem(R=R, dx=dx, m=m, nu=nu, n_steps=n_steps, abc=abc, **kw)
     key_disc = disc_key(R, dx, m, nu)
@@ -85,8 +134,7 @@ def lsq_disc(R, dx, m, nu, n_steps, abc="lsq", **kw):
         raise KeyError(f"no sweep pick tabulated for disc {key_disc}: run python -m lps_b200.configs")
     key = (key_disc, n_steps, tuple(sorted(kw.items())))
     if key not in _cache:
-        _cache[key] = gen.disc_problem(R=R, dx=dx, m=m, nu=nu, n_steps=n_steps, abc="lsq", dt=pick[0],
-                                       dk_factor=pick[1], **kw)
+        _cache[key] = _fitted(R, dx, m, nu, n_steps, pick, kw)
     return _cache[key]
 
 

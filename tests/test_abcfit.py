@@ -63,3 +63,22 @@ def test_fit_rejects_bad_arguments():
     with pytest.raises(ValueError):
         abcfit.fit(np.zeros((4, 2)), np.array([7], np.int32), np.zeros((1, 3), np.int32), E=0.19, nu=0.25,
                    rho=8e-15, delta=2.0, dx=0.5)
+
+
+def test_fit_cache_returns_the_fit(tmp_path, monkeypatch):
+    """The on-disk operator cache (shared by the processes of one host) gives
+    back exactly the operators, time step and fit record that a fresh fit
+    gives, for the second caller as for the first."""
+    from lps_b200 import configs, gen
+    monkeypatch.setenv("LPS_FIT_CACHE", str(tmp_path))
+    pick = (1.75e-8, 0.9)
+    direct = gen.disc_problem(R=10.0, dx=0.5, m=4, nu=0.3, n_steps=20, abc="lsq", dt=pick[0], dk_factor=pick[1],
+                              sigma=3.0)
+    first = configs._fitted(10.0, 0.5, 4, 0.3, 20, pick, {"sigma": 3.0})
+    second = configs._fitted(10.0, 0.5, 4, 0.3, 20, pick, {"sigma": 3.0})
+    assert len(list(tmp_path.glob("*.npz"))) == 1
+    for s in (first, second):
+        for k in ("gu", "gv", "gtheta", "u0", "nodes", "clouds", "inf_nodes", "bctypes"):
+            np.testing.assert_array_equal(getattr(s, k), getattr(direct, k))
+        assert (s.dt, s.t1, s.n_steps) == (direct.dt, direct.t1, direct.n_steps)
+        assert s.fit == direct.fit
