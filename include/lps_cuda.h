@@ -92,8 +92,8 @@ typedef struct lps_options {
   int32_t autotune;         /* 1: lps_create times the dense tile kernels'    */
                             /* step graph at each rows-per-thread choice and  */
                             /* resident-CTA count and keeps the fastest (no   */
-                            /* effect on results); 0 (default): 4 rows, full  */
-                            /* occupancy                                      */
+                            /* effect on results); 0 (default): 4 dilatation */
+                            /* and 2 force rows per thread, full occupancy    */
   int32_t theta_rows;       /* dense dilatation rows per thread: 0 (default:  */
                             /* 4, or the autotuner's choice), 2 or 4 (fixed)  */
   int32_t horizon_build;    /* horizon search (src/main.cpp:352-356): 0 auto  */

@@ -833,11 +833,12 @@ int get_graph(lps_handle *h, int mask, cudaGraphExec_t *out);
 
 // The autotuner of the dense path: for each number of rows a dilatation
 // thread owns (4 and 2; only the requested one when lps_options.theta_rows
-// is set) and every count of resident dilatation / force CTAs per SM (1 up
-// to the occupancy limit) it captures the 12-step CUDA graph the run will
-// replay and times two replays of it from the initial state (the faster of
-// two tries); a choice replaces the default (4 rows, full occupancy) only if
-// it is at least 2 % faster.  None of these changes a result: tiles come from
+// is set), each number of rows a FP32-mixed force thread owns (2 and 4; only
+// the requested one when lps_options.force_rows is set) and every count of
+// resident dilatation / force CTAs per SM (1 up to the occupancy limit) it
+// captures the 12-step CUDA graph the run will replay and times two replays
+// of it from the initial state (the faster of two tries); a choice replaces
+// the default (4 / 2 rows, full occupancy) only if it is at least 2 % faster.  None of these changes a result: tiles come from
 // a counter and each cell's arithmetic is the same whichever CTA and thread
 // computes it.  The caller resets the state afterwards.
 int autotune_dense(lps_handle *h, int rows_only, int force_rows_only) {
